@@ -1,0 +1,227 @@
+/* ref_host.cpp -- ORACLE / TEST INFRASTRUCTURE ONLY.
+ *
+ * Builds the reference's OWN fixed-precision arithmetic for the host CPU:
+ * the mpc_cuda headers include/mpc_cuda/cu_freal.cuh and cu_fcomplex.cuh are
+ * host-capable by design (cu_freal.cuh:23-32 turns __host__/__device__ into
+ * no-ops and uses __uint128_t, cu_freal.cuh:46-47), so this file includes them
+ * straight from the reference tree (-I <reference>/include; nothing is copied)
+ * and exposes the operations the CUDA engine must reproduce through a small
+ * extern "C" surface over AoS arrays of cu_fp::cu_freal<PB> / cu_fcomplex<PB>.
+ *
+ * The result, oracle/_ref/libref_host.so, is the "reference" CPU baseline and a
+ * second, independent check of the C restatement in mpb_oracle.c.  The loops
+ * mirror the reference kernels: demos/bench_3way.cu:44-59 (AXPY),
+ * tools/linalg_fast.cu:37-68 (sequential-k matvec/matmul),
+ * demos/matmul_mpc.cu:39-57 (complex sequential-k order).
+ */
+#include <cstdint>
+#include <cstring>
+#include "mpc_cuda/cu_fcomplex.cuh"
+
+using cu_fp::cu_fcomplex;
+using cu_fp::cu_freal;
+
+namespace {
+
+template <int PB>
+void t_mul(long n, const void *A, const void *B, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto b = (const cu_freal<PB> *)B;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_fmul<PB>(a[i], b[i]);
+}
+template <int PB>
+void t_add(long n, const void *A, const void *B, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto b = (const cu_freal<PB> *)B;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_fadd<PB>(a[i], b[i]);
+}
+template <int PB>
+void t_sub(long n, const void *A, const void *B, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto b = (const cu_freal<PB> *)B;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_fsub<PB>(a[i], b[i]);
+}
+template <int PB>
+void t_cmul(long n, const void *A, const void *B, void *R) {
+  auto a = (const cu_fcomplex<PB> *)A;
+  auto b = (const cu_fcomplex<PB> *)B;
+  auto r = (cu_fcomplex<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_cmul<PB>(a[i], b[i]);
+}
+template <int PB>
+void t_cadd(long n, const void *A, const void *B, void *R) {
+  auto a = (const cu_fcomplex<PB> *)A;
+  auto b = (const cu_fcomplex<PB> *)B;
+  auto r = (cu_fcomplex<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_cadd<PB>(a[i], b[i]);
+}
+template <int PB>
+void t_csub(long n, const void *A, const void *B, void *R) {
+  auto a = (const cu_fcomplex<PB> *)A;
+  auto b = (const cu_fcomplex<PB> *)B;
+  auto r = (cu_fcomplex<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_csub<PB>(a[i], b[i]);
+}
+/* freal_axpy body (demos/bench_3way.cu:47-48): t = a*x; r = t + y */
+template <int PB>
+void t_axpy_r(long n, const void *a, const void *X, const void *Y, void *Z) {
+  const cu_freal<PB> &s = *(const cu_freal<PB> *)a;
+  auto x = (const cu_freal<PB> *)X;
+  auto y = (const cu_freal<PB> *)Y;
+  auto z = (cu_freal<PB> *)Z;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    cu_freal<PB> t = s * x[i];
+    z[i] = t + y[i];
+  }
+}
+/* fcplx_axpy body (demos/bench_3way.cu:55-56) */
+template <int PB>
+void t_axpy_c(long n, const void *a, const void *X, const void *Y, void *Z) {
+  const cu_fcomplex<PB> &s = *(const cu_fcomplex<PB> *)a;
+  auto x = (const cu_fcomplex<PB> *)X;
+  auto y = (const cu_fcomplex<PB> *)Y;
+  auto z = (cu_fcomplex<PB> *)Z;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    cu_fcomplex<PB> t = s * x[i];
+    z[i] = t + y[i];
+  }
+}
+/* matvec_kernel body (tools/linalg_fast.cu:43-48) plus the engine's final +y */
+template <int PB>
+void t_gemv_r(long m, long n, const void *A, long lda, const void *X, const void *Yin, void *Yout) {
+  auto a = (const cu_freal<PB> *)A;
+  auto x = (const cu_freal<PB> *)X;
+  auto yi = (const cu_freal<PB> *)Yin;
+  auto yo = (cu_freal<PB> *)Yout;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long i = 0; i < m; i++) {
+    cu_freal<PB> acc;
+    acc.set_zero();
+    for (long k = 0; k < n; k++) acc = cu_fp::cu_fadd<PB>(acc, cu_fp::cu_fmul<PB>(a[i * lda + k], x[k]));
+    yo[i] = cu_fp::cu_fadd<PB>(acc, yi[i]);
+  }
+}
+template <int PB>
+void t_gemv_c(long m, long n, const void *A, long lda, const void *X, const void *Yin, void *Yout) {
+  auto a = (const cu_fcomplex<PB> *)A;
+  auto x = (const cu_fcomplex<PB> *)X;
+  auto yi = (const cu_fcomplex<PB> *)Yin;
+  auto yo = (cu_fcomplex<PB> *)Yout;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long i = 0; i < m; i++) {
+    cu_fcomplex<PB> acc;
+    acc.re.set_zero();
+    acc.im.set_zero();
+    for (long k = 0; k < n; k++) acc = acc + a[i * lda + k] * x[k];
+    yo[i] = acc + yi[i];
+  }
+}
+/* matmul_kernel body (tools/linalg_fast.cu:59-66), rows [r0, r1) */
+template <int PB>
+void t_gemm_r(long m, long n, long K, const void *A, long lda, const void *B, long ldb, void *C,
+              long ldc, long r0, long r1) {
+  auto a = (const cu_freal<PB> *)A;
+  auto b = (const cu_freal<PB> *)B;
+  auto c = (cu_freal<PB> *)C;
+  if (r1 <= 0 || r1 > m) r1 = m;
+#pragma omp parallel for collapse(2) schedule(dynamic, 16)
+  for (long i = r0; i < r1; i++)
+    for (long j = 0; j < n; j++) {
+      cu_freal<PB> acc;
+      acc.set_zero();
+      for (long k = 0; k < K; k++)
+        acc = cu_fp::cu_fadd<PB>(acc, cu_fp::cu_fmul<PB>(a[i * lda + k], b[k * ldb + j]));
+      c[i * ldc + j] = acc;
+    }
+}
+/* complex sequential-k order of cdot_ij (demos/matmul_mpc.cu:39-57) */
+template <int PB>
+void t_gemm_c(long m, long n, long K, const void *A, long lda, const void *B, long ldb, void *C,
+              long ldc, long r0, long r1) {
+  auto a = (const cu_fcomplex<PB> *)A;
+  auto b = (const cu_fcomplex<PB> *)B;
+  auto c = (cu_fcomplex<PB> *)C;
+  if (r1 <= 0 || r1 > m) r1 = m;
+#pragma omp parallel for collapse(2) schedule(dynamic, 16)
+  for (long i = r0; i < r1; i++)
+    for (long j = 0; j < n; j++) {
+      cu_fcomplex<PB> acc;
+      acc.re.set_zero();
+      acc.im.set_zero();
+      for (long k = 0; k < K; k++) acc = acc + a[i * lda + k] * b[k * ldb + j];
+      c[i * ldc + j] = acc;
+    }
+}
+template <int PB>
+void t_from_double(long n, const double *d, void *R) {
+  auto r = (cu_freal<PB> *)R;
+  for (long i = 0; i < n; i++) r[i] = cu_freal<PB>::from_double(d[i]);
+}
+template <int PB>
+void t_to_double(long n, const void *X, double *d) {
+  auto x = (const cu_freal<PB> *)X;
+  for (long i = 0; i < n; i++) d[i] = x[i].to_double();
+}
+
+/* runtime precision -> template instantiation (the reference's test set,
+ * tools/test_freal.cu:92-102, plus the engine's PB list) */
+#define REF_DISPATCH(P, CALL)                                                                   \
+  switch (P) {                                                                                  \
+    case 32: { constexpr int PB = 32; CALL; } return 0;                                         \
+    case 64: { constexpr int PB = 64; CALL; } return 0;                                         \
+    case 96: { constexpr int PB = 96; CALL; } return 0;                                         \
+    case 128: { constexpr int PB = 128; CALL; } return 0;                                       \
+    case 160: { constexpr int PB = 160; CALL; } return 0;                                       \
+    case 256: { constexpr int PB = 256; CALL; } return 0;                                       \
+    case 288: { constexpr int PB = 288; CALL; } return 0;                                       \
+    case 512: { constexpr int PB = 512; CALL; } return 0;                                       \
+    case 1024: { constexpr int PB = 1024; CALL; } return 0;                                     \
+    case 1056: { constexpr int PB = 1056; CALL; } return 0;                                     \
+    case 2048: { constexpr int PB = 2048; CALL; } return 0;                                     \
+    default: return -1;                                                                         \
+  }
+
+}  // namespace
+
+extern "C" {
+int ref_elem_bytes(int P) { REF_DISPATCH(P, return (int)sizeof(cu_freal<PB>)) }
+int ref_mul(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_mul<PB>(n, A, B, R)) }
+int ref_add(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_add<PB>(n, A, B, R)) }
+int ref_sub(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_sub<PB>(n, A, B, R)) }
+int ref_cmul(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_cmul<PB>(n, A, B, R)) }
+int ref_cadd(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_cadd<PB>(n, A, B, R)) }
+int ref_csub(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_csub<PB>(n, A, B, R)) }
+int ref_axpy_r(int P, long n, const void *a, const void *X, const void *Y, void *Z) {
+  REF_DISPATCH(P, t_axpy_r<PB>(n, a, X, Y, Z))
+}
+int ref_axpy_c(int P, long n, const void *a, const void *X, const void *Y, void *Z) {
+  REF_DISPATCH(P, t_axpy_c<PB>(n, a, X, Y, Z))
+}
+int ref_gemv_r(int P, long m, long n, const void *A, long lda, const void *X, const void *Yi, void *Yo) {
+  REF_DISPATCH(P, t_gemv_r<PB>(m, n, A, lda, X, Yi, Yo))
+}
+int ref_gemv_c(int P, long m, long n, const void *A, long lda, const void *X, const void *Yi, void *Yo) {
+  REF_DISPATCH(P, t_gemv_c<PB>(m, n, A, lda, X, Yi, Yo))
+}
+int ref_gemm_r(int P, long m, long n, long k, const void *A, long lda, const void *B, long ldb,
+               void *C, long ldc, long r0, long r1) {
+  REF_DISPATCH(P, t_gemm_r<PB>(m, n, k, A, lda, B, ldb, C, ldc, r0, r1))
+}
+int ref_gemm_c(int P, long m, long n, long k, const void *A, long lda, const void *B, long ldb,
+               void *C, long ldc, long r0, long r1) {
+  REF_DISPATCH(P, t_gemm_c<PB>(m, n, k, A, lda, B, ldb, C, ldc, r0, r1))
+}
+int ref_from_double(int P, long n, const double *d, void *R) { REF_DISPATCH(P, t_from_double<PB>(n, d, R)) }
+int ref_to_double(int P, long n, const void *X, double *d) { REF_DISPATCH(P, t_to_double<PB>(n, X, d)) }
+}
