@@ -1,0 +1,421 @@
+#!/usr/bin/env python3
+"""bench.py -- throughput of the mpb engine on its benchmark workloads.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpb|reference]
+                    [--workload axpy_c1024|axpy_r256|...]
+
+One JSON line on stdout (rank 0).  A step is one pass of the hot path over
+one batch of synthetic operands already resident in HBM; K steps are timed
+with CUDA events on the launching stream between a barrier and a device
+synchronize, the time is the max over ranks, and ``value`` is the units all
+ranks processed divided by that time.  With N > 1 (torchrun, one process per
+GPU) every rank runs its own independent shard of the same size (weak
+scaling, no data-path collective: the problems are independent).
+
+``e2e`` is the same metric measured through the C ABI starting from HOST
+buffers of mpc_cuda AoS structs (pinned): per step the inputs are copied in,
+packed into the engine layout, computed, unpacked and copied back.
+
+``--impl reference`` times the reference's own implementation of the path on
+the host cores (its cu_freal/cu_fcomplex headers compiled for the CPU with
+OpenMP, oracle/_ref; the oracle's C restatement when that build is absent)
+on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "mp-FMA/s at PB=256/1024: tensor-core exact GEMM vs plain kernel, ≤0.5 ULP"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during timing."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r for r in csv.reader(io.StringIO(self.f.read())) if len(r) >= 9]
+        self.f.close()
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ helpers
+def pinned_from(np_arr):
+    import torch
+
+    t = torch.from_numpy(np_arr.reshape(-1).copy())
+    return t.pin_memory()
+
+
+def dev_from(np_arr, device):
+    import torch
+
+    a = np_arr.reshape(-1)
+    return torch.from_numpy(a.copy()).to(device)
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "MEASURED_PEAKS.json"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def imad_peak(stream_ptr):
+    """IMAD lane-ops/s of this GPU (libmpb_probe.so), or None."""
+    import ctypes
+
+    path = os.path.join(ROOT, "mpc_cuda_b200", "libmpb_probe.so")
+    if not os.path.exists(path):
+        return None
+    L = ctypes.CDLL(path)
+    L.mpb_probe_imad_ops_per_s.argtypes = [ctypes.c_void_p]
+    L.mpb_probe_imad_ops_per_s.restype = ctypes.c_double
+    v = L.mpb_probe_imad_ops_per_s(stream_ptr)
+    return v if v > 0 else None
+
+
+# ------------------------------------------------------------------ workloads
+class AxpyWorkload:
+    """z = a*x + y over n elements (real or complex), rotating input sets so
+    consecutive steps never hit L2 (footprint > 126 MB)."""
+
+    def __init__(self, name, cplx, prec, n, seed):
+        self.name, self.cplx, self.prec, self.n, self.seed = name, cplx, prec, n, seed
+        comp = 2 if cplx else 1
+        self.elem_bytes = comp * 4 * (prec // 32 + 1)  # tiled layout, limbs + head
+        # one complex mp-FMA = one complex multiply (4 exact products) + add
+        self.products = 4 if cplx else 1
+        self.nsets = max(2, -(-2 * L2_BYTES // (3 * n * self.elem_bytes)))
+        self.desc = (f"{'complex' if cplx else 'real'} AXPY z=a*x+y, "
+                     f"{'cu_fcomplex' if cplx else 'cu_freal'}<{prec}>, "
+                     f"{'MPC_RNDNN' if cplx else 'RNDN'} per operation, n=2^{n.bit_length() - 1}")
+
+    def make_host(self, rank):
+        from mpc_cuda_b200 import layout, synth
+
+        if self.cplx:
+            a, x, y = synth.axpy_c1024(seed=self.seed + 1000 * rank, n=self.n, prec=self.prec)
+            conv = lambda p: synth.interleave_complex(self.prec, *p)  # noqa: E731
+        else:
+            a, x, y = synth.axpy_r256(seed=self.seed + 1000 * rank, n=self.n, prec=self.prec)
+            conv = lambda p: layout.aos_from_parts(self.prec, *p)  # noqa: E731
+        return conv(a), conv(x), conv(y)
+
+    def setup(self, rank, device):
+        import mpc_cuda_b200 as M
+        from mpc_cuda_b200 import layout
+
+        self.M = M
+        A, X, Y = self.make_host(rank)
+        self.host = (A, X, Y)
+        vec = lambda aos: dev_from(layout.aos_to_vec(self.prec, aos, self.cplx), device)  # noqa: E731
+        self.a = vec(A)
+        self.sets = []
+        for s in range(self.nsets):
+            xs = vec(X) if s == 0 else self.sets[0][0].clone()
+            ys = vec(Y) if s == 0 else self.sets[0][1].clone()
+            self.sets.append((xs, ys, M.empty(self.prec, self.n, self.cplx, device=device)))
+        # e2e: pinned host AoS buffers and device staging
+        import torch
+
+        self.hx, self.hy = pinned_from(X), pinned_from(Y)
+        self.hz = torch.empty(X.size, dtype=torch.uint8).pin_memory()
+        self.dx_aos = torch.empty(X.size, dtype=torch.uint8, device=device)
+        self.dy_aos = torch.empty(Y.size, dtype=torch.uint8, device=device)
+        self.dz_aos = torch.empty(X.size, dtype=torch.uint8, device=device)
+        self.ex, self.ey, self.ez = (M.empty(self.prec, self.n, self.cplx, device=device) for _ in range(3))
+
+    def units(self):
+        return self.n
+
+    def step(self, i, stream):
+        x, y, z = self.sets[i % self.nsets]
+        self.M.axpy(self.prec, self.n, self.a, x, y, z, self.cplx, stream=stream)
+
+    launches_per_step = 1
+
+    def e2e_step(self, i, stream):
+        M = self.M
+        self.dx_aos.copy_(self.hx, non_blocking=True)
+        self.dy_aos.copy_(self.hy, non_blocking=True)
+        M.pack_aos(self.prec, self.n, self.dx_aos, self.ex, self.cplx, stream=stream)
+        M.pack_aos(self.prec, self.n, self.dy_aos, self.ey, self.cplx, stream=stream)
+        M.axpy(self.prec, self.n, self.a, self.ex, self.ey, self.ez, self.cplx, stream=stream)
+        M.unpack_aos(self.prec, self.n, self.ez, self.dz_aos, self.cplx, stream=stream)
+        self.hz.copy_(self.dz_aos, non_blocking=True)
+
+    e2e_launches_per_step = 4
+
+    def e2e_bytes(self):
+        return 2 * self.host[1].size, self.host[1].size
+
+    def roofline(self, kernel_s, peaks, imad_ops_s):
+        N = self.prec // 32
+        imad_per_unit = self.products * 2 * N * N  # schoolbook lo+hi multiply-adds
+        bytes_per_unit = 3 * self.elem_bytes
+        imad = imad_per_unit * self.n / kernel_s
+        gbs = bytes_per_unit * self.n / kernel_s / 1e9
+        hbm_peak, hbm_src = peaks
+        hbm = {"achieved": round(gbs, 1), "peak": hbm_peak["hbm_gbs"], "unit": "GB/s",
+               "frac": round(gbs / hbm_peak["hbm_gbs"], 4), "bytes_per_unit": bytes_per_unit,
+               "peak_source": hbm_src}
+        if self.prec <= 256 and not self.cplx or imad_ops_s is None:
+            out = {"bound": "hbm", **hbm, "traffic": None}
+            out["imad"] = None if imad_ops_s is None else {
+                "achieved": round(imad / 1e9, 1), "peak": round(imad_ops_s / 1e9, 1), "unit": "Gop/s",
+                "frac": round(imad / imad_ops_s, 4), "ops_per_unit": imad_per_unit}
+            return out
+        return {"bound": "imad", "achieved": round(imad / 1e9, 1), "peak": round(imad_ops_s / 1e9, 1),
+                "unit": "Gop/s", "frac": round(imad / imad_ops_s, 4), "ops_per_unit": imad_per_unit,
+                "peak_source": "libmpb_probe.so mad.lo/mad.hi throughput, measured in this run",
+                "traffic": None, "hbm": hbm}
+
+    def cpu_run(self, impl, count):
+        import oracle as O
+
+        A, X, Y = self.host
+        return O.axpy(self.prec, A, X[:count], Y[:count], self.cplx, impl=impl)
+
+    def config(self):
+        return {"workload": self.desc, "prec": self.prec, "n": self.n,
+                "units": "complex mp-FMA (one complex multiply + one complex add)" if self.cplx
+                else "mp-FMA (one multiply + one add, each rounded)",
+                "layout": "tiled SoL, 32-element tiles, 128-bit limb groups + 32-bit head",
+                "l2": f"{self.nsets} rotating input sets, {self.nsets * 3 * self.n * self.elem_bytes >> 20} MiB > L2"}
+
+
+WORKLOADS = {
+    "axpy_c1024": lambda: AxpyWorkload("axpy_c1024", True, 1024, 1 << 18, 0x5EED2),
+    "axpy_r256": lambda: AxpyWorkload("axpy_r256", False, 256, 1 << 20, 0x5EED1),
+}
+DEFAULT_WORKLOAD = "axpy_c1024"
+
+
+# ------------------------------------------------------------------ CPU side
+def cpu_baseline(wl, max_seconds=15.0):
+    """Time the reference's CPU implementation on a bounded sample."""
+    import oracle as O
+
+    impl, kind = ("ref", "reference") if O.ref_available() else ("orc", "port")
+    n_total = wl.units()
+    count = min(n_total, 2048)
+    t0 = time.perf_counter()
+    wl.cpu_run(impl, count)
+    dt = time.perf_counter() - t0
+    target = min(n_total, max(count, int(count * (max_seconds / 3) / max(dt, 1e-6))))
+    t0 = time.perf_counter()
+    wl.cpu_run(impl, target)
+    dt = time.perf_counter() - t0
+    src = ("reference headers include/mpc_cuda/cu_freal.cuh + cu_fcomplex.cuh built for the host "
+           "(oracle/_ref), OpenMP" if kind == "reference" else "oracle C restatement, OpenMP")
+    return {"value": target / dt, "unit": "mp-FMA/s", "cores": O.num_threads(), "kind": kind,
+            "sample": f"{target} of {n_total} elements of the same workload, {dt:.2f} s; {src}"}
+
+
+def run_reference(args):
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    wl = WORKLOADS[args.workload]()
+    wl.host = wl.make_host(0)
+    import oracle as O
+
+    impl, kind = ("ref", "reference") if O.ref_available() else ("orc", "port")
+    count = min(wl.units(), 2048)
+    t0 = time.perf_counter()
+    wl.cpu_run(impl, count)
+    dt = time.perf_counter() - t0
+    per_step = min(wl.units(), max(count, int(count * 8.0 / max(args.steps + args.warmup, 1) / max(dt, 1e-6))))
+    for _ in range(args.warmup):
+        wl.cpu_run(impl, per_step)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        wl.cpu_run(impl, per_step)
+    dt = time.perf_counter() - t0
+    value = per_step * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "mp-FMA/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic", "config": wl.config(),
+        "cpu_baseline": {"value": value, "unit": "mp-FMA/s", "cores": O.num_threads(), "kind": kind,
+                         "sample": f"{per_step} of {wl.units()} elements per step"},
+        "e2e": {"value": value, "unit": "mp-FMA/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU side
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    wl = WORKLOADS[args.workload]()
+    wl.setup(rank, device)
+    stream = torch.cuda.current_stream(device)
+    sp = stream.cuda_stream
+
+    for i in range(args.warmup):
+        wl.step(i, sp)
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local) if rank == 0 else None
+    barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        wl.step(i, sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    barrier()
+    clk = clocks.stop() if clocks else None
+    ms_max = max_over_ranks(ms)
+    kernel_s = ms / args.steps / 1e3
+
+    # end to end through the C ABI from host AoS buffers
+    for i in range(max(1, args.warmup)):
+        wl.e2e_step(i, sp)
+    torch.cuda.synchronize()
+    barrier()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for i in range(args.steps):
+        wl.e2e_step(i, sp)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(e2.elapsed_time(e3))
+    barrier()
+
+    units = wl.units() * world * args.steps
+    if rank == 0:
+        peaks = measured_peaks()
+        ipk = imad_peak(sp)
+        roof = wl.roofline(kernel_s, peaks, ipk)
+        cpu = cpu_baseline(wl) if world == 1 else None
+        h2d, d2h = wl.e2e_bytes()
+        line = {
+            "metric": METRIC, "value": units / (ms_max / 1e3), "unit": "mp-FMA/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "config": {**wl.config(), "parallelism": f"{world} independent shard(s), "
+                                                                          "no collective"},
+            "roofline": roof, "cpu_baseline": cpu,
+            "e2e": {"value": units / (ms_e2e / 1e3), "unit": "mp-FMA/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps,
+                    "path": "pinned host AoS -> H2D -> mpb_pack_aos -> kernel -> mpb_unpack_aos -> D2H"},
+            "gpu_launches": wl.launches_per_step * args.steps,
+            "gpu_launches_e2e": wl.e2e_launches_per_step * args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("mpb", "reference"), default="mpb")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

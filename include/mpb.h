@@ -1,0 +1,107 @@
+/* mpb.h -- C ABI of the mpb B200 fixed-precision linear-algebra engine.
+ *
+ * Plain C: int precision, size_t sizes, void pointers, an opaque stream
+ * (a cudaStream_t passed as void*, NULL = the legacy default stream).  No
+ * allocation, no host synchronisation: every call validates its arguments on
+ * the host, enqueues its kernels on `stream` and returns.
+ *
+ * Precisions: prec in {64, 128, 256, 512, 1024, 2048} bits.
+ * Rounding: round-to-nearest-even after every operation, bit-exact with MPFR
+ * (real, MPFR_RNDN) and MPC (complex, MPC_RNDNN); zero results are +0.
+ *
+ * Data layout (device buffers, "SoL tiles", see mpb/layout.cuh): a real
+ * vector of n elements occupies mpb_vec_bytes(prec, n) bytes, a complex one
+ * mpb_cvec_bytes(prec, n); buffers must be 16-byte aligned.  Matrices are
+ * row-major with a leading dimension ld that is a multiple of 32 elements.
+ * Conversions to and from the mpc_cuda AoS structs (cu_fp::cu_freal<prec>,
+ * cu_fp::cu_fcomplex<prec>) and from/to double are provided on the device.
+ *
+ * Every entry point returns MPB_OK (0) or a negative mpb_status.  n == 0 (or
+ * an empty matrix) is a valid no-op.
+ *
+ * Each declaration names the mpc_cuda code whose behaviour it provides.
+ */
+#ifndef MPB_H
+#define MPB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  MPB_OK = 0,
+  MPB_ERR_PREC = -1,     /* precision not in the supported set */
+  MPB_ERR_SIZE = -2,     /* size overflows the addressable range */
+  MPB_ERR_NULL = -3,     /* a required pointer is NULL */
+  MPB_ERR_ALIGN = -4,    /* a device buffer is not 16-byte aligned */
+  MPB_ERR_LD = -5,       /* leading dimension not a multiple of 32 or too small */
+  MPB_ERR_CUDA = -6,     /* a CUDA launch or runtime call failed */
+  MPB_ERR_ARG = -7,      /* any other invalid argument */
+  MPB_ERR_WORKSPACE = -8 /* workspace missing or too small */
+} mpb_status;
+
+typedef enum { MPB_OP_MUL = 0, MPB_OP_ADD = 1, MPB_OP_SUB = 2 } mpb_op;
+
+/* ---- library information ---- */
+int mpb_version(void);                         /* major*10000 + minor*100 + patch */
+const char *mpb_status_string(int status);
+int mpb_prec_supported(int prec);              /* 1 if prec is one of the supported values */
+
+/* ---- layout ---- */
+size_t mpb_vec_bytes(int prec, size_t n);      /* real vector, 0 for unsupported prec */
+size_t mpb_cvec_bytes(int prec, size_t n);     /* complex vector */
+size_t mpb_aos_bytes(int prec);                /* sizeof(cu_fp::cu_freal<prec>) (reference cu_freal.cuh:67-77) */
+
+/* AoS cu_freal<prec>[n] (device) <-> tiled vector (device).
+ * Replaces building/reading cu_freal arrays in place (reference cu_freal.cuh:67-81,
+ * tools/test_freal.cu:56-67 copies AoS structs to and from the device). */
+int mpb_pack_aos(int prec, size_t n, const void *aos, void *vec, void *stream);
+int mpb_unpack_aos(int prec, size_t n, const void *vec, void *aos, void *stream);
+/* AoS cu_fcomplex<prec>[n] <-> complex tiled vector (reference cu_fcomplex.cuh:98-113) */
+int mpb_cpack_aos(int prec, size_t n, const void *aos, void *cvec, void *stream);
+int mpb_cunpack_aos(int prec, size_t n, const void *cvec, void *aos, void *stream);
+/* double[n] -> vector, exact (reference cu_freal<PB>::from_double, cu_freal.cuh:141-149) */
+int mpb_from_double(int prec, size_t n, const double *d, void *vec, void *stream);
+/* vector -> double[n], RNDN (reference cu_freal<PB>::to_double, cu_freal.cuh:150-165) */
+int mpb_to_double(int prec, size_t n, const void *vec, double *d, void *stream);
+
+/* ---- element-wise operators ---- */
+/* r[i] = a[i] op b[i]  (reference operators * + -, cu_freal.cuh:358-364; cu_fmul/cu_fadd/cu_fsub) */
+int mpb_binop_r(int prec, int op, size_t n, const void *a, const void *b, void *r, void *stream);
+/* r[i] = round(a[i]*b[i] + c[i]), one rounding (mpfr_fma; no counterpart in the reference) */
+int mpb_fma_r(int prec, size_t n, const void *a, const void *b, const void *c, void *r, void *stream);
+/* complex r[i] = a[i] op b[i] (reference cu_cmul/cu_cadd/cu_csub, cu_fcomplex.cuh:115-131) */
+int mpb_binop_c(int prec, int op, size_t n, const void *a, const void *b, void *r, void *stream);
+
+/* ---- AXPY ---- */
+/* z[i] = round(round(a*x[i]) + y[i]); a is element 0 of a real vector
+ * (reference freal_axpy, demos/bench_3way.cu:44-50) */
+int mpb_axpy_r(int prec, size_t n, const void *a, const void *x, const void *y, void *z, void *stream);
+/* complex z[i] = a*x[i] + y[i], MPC_RNDNN per operation
+ * (reference fcplx_axpy, demos/bench_3way.cu:51-59; axpyc, tools/axpy_fast_complex.cu:32-40) */
+int mpb_axpy_c(int prec, size_t n, const void *a, const void *x, const void *y, void *z, void *stream);
+
+/* ---- GEMV / GEMM, per-operation rounding in sequential k order ---- */
+/* y_out[i] = round(dot_i + y[i]), dot_i: acc = +0; acc = round(acc + round(A[i,k]*x[k])), k = 0..n-1.
+ * A is m x n (row-major, lda).  y_out may alias y.
+ * (reference matvec_kernel, tools/linalg_fast.cu:37-51, which has no "+ y") */
+int mpb_gemv_r(int prec, size_t m, size_t n, const void *A, size_t lda, const void *x, const void *y,
+               void *y_out, void *stream);
+int mpb_gemv_c(int prec, size_t m, size_t n, const void *A, size_t lda, const void *x, const void *y,
+               void *y_out, void *stream);
+/* C[i,j] = sequential-k dot of row i of A (m x k) and column j of B (k x n)
+ * (reference matmul_kernel, tools/linalg_fast.cu:53-68; complex order of
+ * cdot_ij, demos/matmul_mpc.cu:39-57) */
+int mpb_gemm_r(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
+               void *C, size_t ldc, void *stream);
+int mpb_gemm_c(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
+               void *C, size_t ldc, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPB_H */

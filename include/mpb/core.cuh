@@ -1,0 +1,489 @@
+/* mpb/core.cuh -- register-resident fixed-precision limb arithmetic for sm_100a
+ * (and, through the same code, for the host CPU).
+ *
+ * A value with N 32-bit limbs (precision PB = 32*N bits) is
+ *     value = (-1)^s * M * 2^(e - 32*N),   M = sum m[i] * 2^(32 i)
+ * with M left-justified (bit 31 of m[N-1] set) unless the value is zero, in
+ * which case e == kExpZero and every limb is 0.  e is the MPFR exponent, so an
+ * N-limb value has exactly the significand and exponent MPFR stores for the
+ * same number at PB bits (MPFR limbs are 64-bit; their 32-bit halves are these
+ * limbs), and exactly those of the mpc_cuda cu_freal<PB> struct.
+ *
+ * Every operation is round-to-nearest-even (MPFR_RNDN) with one rounding per
+ * operation:
+ *   mul          round(a*b)                (full N x N -> 2N product)
+ *   add_round    round(x + y)              (x, y exact NX-limb terms, result NM limbs)
+ *   fma          round(a*b + c)            (single rounding)
+ *   fmms/fmma    round(a*b -/+ c*d)        (single rounding; complex multiply)
+ * Zero is unsigned (+0), as in cu_freal (cu_freal.cuh:79-81 of mpc_cuda).
+ *
+ * B200 design points:
+ *  - 32-bit limbs: the integer datapath is 32 bits wide (IMAD / IMAD.HI with
+ *    carry), 64-bit limbs would be emulated.
+ *  - Products use PTX carry chains (mad.lo.cc / madc.hi.cc) - 2N^2+N IMADs.
+ *  - No runtime-indexed local arrays: every shift (alignment, normalisation)
+ *    is a compile-time-unrolled log-depth network of predicated selects and
+ *    funnel shifts, so all limbs stay in registers.
+ *  - Kernels that keep their warps converged may pass kVote=true, which lets a
+ *    warp skip the rare normalisation/negation networks when no lane needs them.
+ *
+ * The host build emulates each PTX carry-chain instruction with an explicit
+ * carry flag (same call sequence), so the chain logic is exercised by CPU
+ * tests against MPFR.
+ */
+#ifndef MPB_CORE_CUH
+#define MPB_CORE_CUH
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define MPB_HD __host__ __device__ __forceinline__
+#define MPB_HDI __host__ __device__ inline
+#else
+#define MPB_HD inline
+#define MPB_HDI inline
+#endif
+
+#if defined(__CUDACC__)
+#define MPB_UNROLL _Pragma("unroll")
+#else
+#define MPB_UNROLL
+#endif
+
+namespace mpb {
+
+/* exponent of zero: below MPFR's default emin (1 - 2^30) */
+constexpr int32_t kExpZero = -(1 << 30);
+
+template <int N>
+struct fval {
+  uint32_t m[N];
+  int32_t e;
+  uint32_t s; /* 1 = negative */
+};
+
+/* ------------------------------------------------------------------ *
+ * carry-chain primitives.  cf is the carry flag; on the device it is
+ * the hardware CC.CF and the argument is unused.
+ * ------------------------------------------------------------------ */
+#if defined(__CUDA_ARCH__)
+MPB_HD uint32_t cc_set(uint32_t cin, uint32_t &) { /* CF = (cin != 0), cin in {0,1} */
+  uint32_t d;
+  asm volatile("add.cc.u32 %0, %1, 0xffffffff;" : "=r"(d) : "r"(cin));
+  return d;
+}
+MPB_HD uint32_t add_cc(uint32_t a, uint32_t b, uint32_t &) {
+  uint32_t d;
+  asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+MPB_HD uint32_t addc_cc(uint32_t a, uint32_t b, uint32_t &) {
+  uint32_t d;
+  asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+MPB_HD uint32_t addc(uint32_t a, uint32_t b, uint32_t &) {
+  uint32_t d;
+  asm volatile("addc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+MPB_HD uint32_t madlo_cc(uint32_t a, uint32_t b, uint32_t c, uint32_t &) {
+  uint32_t d;
+  asm volatile("mad.lo.cc.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+MPB_HD uint32_t madclo_cc(uint32_t a, uint32_t b, uint32_t c, uint32_t &) {
+  uint32_t d;
+  asm volatile("madc.lo.cc.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+MPB_HD uint32_t madhi_cc(uint32_t a, uint32_t b, uint32_t c, uint32_t &) {
+  uint32_t d;
+  asm volatile("mad.hi.cc.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+MPB_HD uint32_t madchi_cc(uint32_t a, uint32_t b, uint32_t c, uint32_t &) {
+  uint32_t d;
+  asm volatile("madc.hi.cc.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+MPB_HD uint32_t madchi(uint32_t a, uint32_t b, uint32_t c, uint32_t &) {
+  uint32_t d;
+  asm volatile("madc.hi.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+MPB_HD uint32_t mulhi(uint32_t a, uint32_t b) { return __umulhi(a, b); }
+MPB_HD uint32_t fshl(uint32_t lo, uint32_t hi, uint32_t s) { return __funnelshift_l(lo, hi, s); }
+MPB_HD uint32_t fshr(uint32_t lo, uint32_t hi, uint32_t s) { return __funnelshift_r(lo, hi, s); }
+MPB_HD uint32_t clz32(uint32_t x) { return (uint32_t)__clz(x); }
+#else
+MPB_HD uint32_t cc_set(uint32_t cin, uint32_t &cf) {
+  cf = cin ? 1u : 0u;
+  return cin + 0xffffffffu;
+}
+MPB_HD uint32_t add_cc(uint32_t a, uint32_t b, uint32_t &cf) {
+  uint64_t t = (uint64_t)a + b;
+  cf = (uint32_t)(t >> 32);
+  return (uint32_t)t;
+}
+MPB_HD uint32_t addc_cc(uint32_t a, uint32_t b, uint32_t &cf) {
+  uint64_t t = (uint64_t)a + b + cf;
+  cf = (uint32_t)(t >> 32);
+  return (uint32_t)t;
+}
+MPB_HD uint32_t addc(uint32_t a, uint32_t b, uint32_t &cf) { return a + b + cf; }
+MPB_HD uint32_t madlo_cc(uint32_t a, uint32_t b, uint32_t c, uint32_t &cf) {
+  uint64_t t = (uint64_t)(uint32_t)(a * b) + c;
+  cf = (uint32_t)(t >> 32);
+  return (uint32_t)t;
+}
+MPB_HD uint32_t madclo_cc(uint32_t a, uint32_t b, uint32_t c, uint32_t &cf) {
+  uint64_t t = (uint64_t)(uint32_t)(a * b) + c + cf;
+  cf = (uint32_t)(t >> 32);
+  return (uint32_t)t;
+}
+MPB_HD uint32_t madhi_cc(uint32_t a, uint32_t b, uint32_t c, uint32_t &cf) {
+  uint64_t t = (((uint64_t)a * b) >> 32) + c;
+  cf = (uint32_t)(t >> 32);
+  return (uint32_t)t;
+}
+MPB_HD uint32_t madchi_cc(uint32_t a, uint32_t b, uint32_t c, uint32_t &cf) {
+  uint64_t t = (((uint64_t)a * b) >> 32) + c + cf;
+  cf = (uint32_t)(t >> 32);
+  return (uint32_t)t;
+}
+MPB_HD uint32_t madchi(uint32_t a, uint32_t b, uint32_t c, uint32_t &cf) {
+  return (uint32_t)(((uint64_t)a * b) >> 32) + c + cf;
+}
+MPB_HD uint32_t mulhi(uint32_t a, uint32_t b) { return (uint32_t)(((uint64_t)a * b) >> 32); }
+MPB_HD uint32_t fshl(uint32_t lo, uint32_t hi, uint32_t s) {
+  return (uint32_t)((((uint64_t)hi << 32) | lo) << (s & 31) >> 32);
+}
+MPB_HD uint32_t fshr(uint32_t lo, uint32_t hi, uint32_t s) {
+  return (uint32_t)((((uint64_t)hi << 32) | lo) >> (s & 31));
+}
+MPB_HD uint32_t clz32(uint32_t x) { return x ? (uint32_t)__builtin_clz(x) : 32u; }
+#endif
+
+/* warp-uniform "does any lane need this" vote (device, converged warps only) */
+template <bool kVote>
+MPB_HD bool any_lane(bool p) {
+#if defined(__CUDA_ARCH__)
+  if (kVote) return __any_sync(0xffffffffu, p);
+#endif
+  return p;
+}
+
+/* ------------------------------------------------------------------ *
+ * exact N x N -> 2N product, schoolbook over PTX carry chains.
+ * Row j adds lo(a*b[j]) at offset j (one chain) and hi(a*b[j]) at
+ * offset j+1 (a second chain); 2N^2 + N multiply-adds in total.
+ * ------------------------------------------------------------------ */
+template <int N>
+MPB_HD void mul_full(uint32_t *p, const uint32_t *a, const uint32_t *b) {
+  uint32_t cf = 0;
+  const uint32_t b0 = b[0];
+  MPB_UNROLL
+  for (int i = 0; i < N; ++i) p[i] = a[i] * b0;
+  if (N == 1) {
+    p[1] = mulhi(a[0], b0);
+    return;
+  }
+  p[1] = madhi_cc(a[0], b0, p[1], cf);
+  MPB_UNROLL
+  for (int i = 1; i < N - 1; ++i) p[i + 1] = madchi_cc(a[i], b0, p[i + 1], cf);
+  p[N] = madchi(a[N - 1], b0, 0u, cf);
+  MPB_UNROLL
+  for (int j = 1; j < N; ++j) {
+    const uint32_t bj = b[j];
+    p[j] = madlo_cc(a[0], bj, p[j], cf);
+    MPB_UNROLL
+    for (int i = 1; i < N; ++i) p[i + j] = madclo_cc(a[i], bj, p[i + j], cf);
+    p[j + N] = addc(0u, 0u, cf);
+    p[j + 1] = madhi_cc(a[0], bj, p[j + 1], cf);
+    MPB_UNROLL
+    for (int i = 1; i < N - 1; ++i) p[i + j + 1] = madchi_cc(a[i], bj, p[i + j + 1], cf);
+    p[j + N] = madchi(a[N - 1], bj, p[j + N], cf);
+  }
+}
+
+/* m[0..n) += inc (inc in {0,1}); returns the carry out */
+template <int n>
+MPB_HD uint32_t inc_n(uint32_t *m, uint32_t inc) {
+  uint32_t cf = 0;
+  m[0] = add_cc(m[0], inc, cf);
+  MPB_UNROLL
+  for (int i = 1; i < n; ++i) m[i] = addc_cc(m[i], 0u, cf);
+  return addc(0u, 0u, cf);
+}
+
+/* Round-to-nearest-even increment of the NM-limb mantissa m given the round
+ * bit rb and a nonzero-if-sticky word st; renormalises on carry-out. */
+template <int NM>
+MPB_HD void rndn(uint32_t *m, int32_t &e, uint32_t rb, uint32_t st) {
+  const uint32_t inc = rb & ((st != 0u) | (m[0] & 1u));
+  const uint32_t c = inc_n<NM>(m, inc);
+  m[NM - 1] |= c << 31; /* all-ones + 1 -> 1000...0 */
+  e += (int32_t)c;
+}
+
+/* ------------------------------------------------------------------ *
+ * r = round(a * b)
+ * ------------------------------------------------------------------ */
+/* Round an exact normalised-or-half-normalised 2N-limb product p (leading
+ * one at bit 64N-1 or 64N-2) with exponent e (for the 64N-1 case) to N limbs. */
+template <int N>
+MPB_HD void round_prod(fval<N> &r, const uint32_t *p, int32_t e, uint32_t s) {
+  const uint32_t sh = (p[2 * N - 1] >> 31) ^ 1u;
+  MPB_UNROLL
+  for (int i = 0; i < N; ++i) r.m[i] = fshl(p[N + i - 1], p[N + i], sh);
+  const uint32_t below = (N >= 2) ? p[N - 2] : 0u;
+  const uint32_t low = fshl(below, p[N - 1], sh);
+  uint32_t st = low << 1;
+  MPB_UNROLL
+  for (int i = 0; i < N - 1; ++i) st |= p[i];
+  r.e = e - (int32_t)sh;
+  rndn<N>(r.m, r.e, low >> 31, st);
+  r.s = s;
+}
+
+template <int N>
+MPB_HD void set_zero(fval<N> &r) {
+  MPB_UNROLL
+  for (int i = 0; i < N; ++i) r.m[i] = 0u;
+  r.e = kExpZero;
+  r.s = 0u;
+}
+template <int N>
+MPB_HD bool is_zero(const fval<N> &x) {
+  return x.e == kExpZero;
+}
+
+template <int N>
+MPB_HD void mul(fval<N> &r, const fval<N> &a, const fval<N> &b) {
+  uint32_t p[2 * N];
+  mul_full<N>(p, a.m, b.m);
+  round_prod<N>(r, p, a.e + b.e, a.s ^ b.s);
+  if (is_zero(a) || is_zero(b)) set_zero(r);
+}
+
+/* exact product, normalised so that bit 31 of p[2N-1] is set (zero stays 0) */
+template <int N>
+MPB_HD void mul_exact_norm(uint32_t *p, int32_t &e, const fval<N> &a, const fval<N> &b) {
+  mul_full<N>(p, a.m, b.m);
+  const uint32_t sh = (p[2 * N - 1] >> 31) ^ 1u;
+  MPB_UNROLL
+  for (int i = 2 * N - 1; i > 0; --i) p[i] = fshl(p[i - 1], p[i], sh);
+  p[0] <<= sh;
+  e = a.e + b.e - (int32_t)sh;
+  if (is_zero(a) || is_zero(b)) e = kExpZero;
+}
+
+/* ------------------------------------------------------------------ *
+ * r = round(x + y) for exact NX-limb terms x, y (each normalised, or zero
+ * with kExpZero and zero limbs), rounded once to NM <= NX limbs.
+ *
+ * Window of W = NX + 2 limbs: the larger-exponent term sits in the top NX
+ * limbs, the other is shifted right by the exponent difference d; bits that
+ * fall below the window only matter as sticky.  For opposite signs, a sticky
+ * window makes the window difference one unit too large, so one unit is
+ * subtracted (borrow-in) and sticky stays set; the cancellation can then be
+ * at most one bit (d >= 2), well inside the 64-bit guard.  A negative window
+ * difference (possible only for d = 0) is negated exactly.
+ * ------------------------------------------------------------------ */
+template <int W>
+struct log2_ceil {
+  static constexpr int v = (W <= 1) ? 0 : 1 + log2_ceil<(W + 1) / 2>::v;
+};
+template <>
+struct log2_ceil<1> {
+  static constexpr int v = 0;
+};
+
+template <int NX, int NM, bool kVote = false>
+MPB_HD void add_round(fval<NM> &r, const uint32_t *xm, int32_t xe, uint32_t xs,
+                      const uint32_t *ym, int32_t ye, uint32_t ys) {
+  constexpr int W = NX + 2;
+  constexpr int KQ = log2_ceil<W + 1>::v; /* limb-shift stages: 2^KQ > W */
+  const bool sw = ye > xe;
+  uint32_t D[W + 1], Y[W];
+  D[0] = 0u;
+  D[1] = 0u;
+  Y[0] = 0u;
+  Y[1] = 0u;
+  MPB_UNROLL
+  for (int i = 0; i < NX; ++i) {
+    D[i + 2] = sw ? ym[i] : xm[i];
+    Y[i + 2] = sw ? xm[i] : ym[i];
+  }
+  const int32_t ea = sw ? ye : xe;
+  const int32_t eb = sw ? xe : ye;
+  const uint32_t sa = sw ? ys : xs;
+  const uint32_t sb = sw ? xs : ys;
+
+  /* ---- align Y right by d = ea - eb bits (limb part q, bit part rs) ---- */
+  const uint32_t d = (uint32_t)(ea - eb);
+  const uint32_t q = (d >> 5) < (uint32_t)W ? (d >> 5) : (uint32_t)W;
+  const uint32_t rs = d & 31u;
+  uint32_t st = 0u;
+  MPB_UNROLL
+  for (int k = 0; k < KQ; ++k) {
+    constexpr int dummy = 0;
+    (void)dummy;
+    const int sh = 1 << k;
+    const bool on = (q >> k) & 1u;
+    uint32_t lost = 0u;
+    MPB_UNROLL
+    for (int i = 0; i < sh && i < W; ++i) lost |= Y[i];
+    st |= on ? lost : 0u;
+    MPB_UNROLL
+    for (int i = 0; i < W; ++i) {
+      const uint32_t src = (i + sh < W) ? Y[i + sh] : 0u;
+      Y[i] = on ? src : Y[i];
+    }
+  }
+  st |= Y[0] & ((1u << rs) - 1u);
+  MPB_UNROLL
+  for (int i = 0; i < W - 1; ++i) Y[i] = fshr(Y[i], Y[i + 1], rs);
+  Y[W - 1] >>= rs;
+
+  /* ---- D = X + Y   or   X - Y - sticky ---- */
+  const uint32_t sub = sa ^ sb;
+  const uint32_t msk = 0u - sub;
+  const uint32_t cin = sub & (st == 0u ? 1u : 0u);
+  uint32_t cf = 0;
+  cc_set(cin, cf);
+  MPB_UNROLL
+  for (int i = 0; i < W; ++i) D[i] = addc_cc(D[i], Y[i] ^ msk, cf);
+  const uint32_t c = addc(0u, 0u, cf);
+
+  /* negative difference (d == 0 and |y| > |x|): negate exactly */
+  const uint32_t neg = sub & (c ^ 1u);
+  if (any_lane<kVote>(neg != 0u)) {
+    const uint32_t nm = 0u - neg;
+    uint32_t cf2 = 0;
+    cc_set(neg, cf2);
+    MPB_UNROLL
+    for (int i = 0; i < W; ++i) D[i] = addc_cc(D[i] ^ nm, 0u, cf2);
+  }
+  uint32_t s = sa ^ neg;
+
+  /* same-sign carry-out: shift right by one, the lost bit joins sticky */
+  const uint32_t cs = (sub ^ 1u) & c;
+  st |= D[0] & cs;
+  D[W] = c;
+  MPB_UNROLL
+  for (int i = 0; i < W; ++i) D[i] = fshr(D[i], D[i + 1], cs);
+
+  /* ---- normalise left (cancellation after subtraction) ---- */
+  uint32_t lq = (uint32_t)W, top = 0u;
+  MPB_UNROLL
+  for (int i = W - 1; i >= 0; --i) {
+    const bool take = (lq == (uint32_t)W) && (D[i] != 0u);
+    top = take ? D[i] : top;
+    lq = take ? (uint32_t)(W - 1 - i) : lq;
+  }
+  const bool zero = (lq == (uint32_t)W);
+  const uint32_t lr = clz32(top) & 31u;
+  if (any_lane<kVote>(lq != 0u && !zero)) {
+    const uint32_t qq = zero ? 0u : lq;
+    MPB_UNROLL
+    for (int k = 0; k < KQ; ++k) {
+      const int sh = 1 << k;
+      const bool on = (qq >> k) & 1u;
+      MPB_UNROLL
+      for (int i = W - 1; i >= 0; --i) {
+        const uint32_t src = (i - sh >= 0) ? D[i - sh] : 0u;
+        D[i] = on ? src : D[i];
+      }
+    }
+  }
+  MPB_UNROLL
+  for (int i = W - 1; i > 0; --i) D[i] = fshl(D[i - 1], D[i], lr);
+  D[0] <<= lr;
+
+  /* ---- round to NM limbs ---- */
+  MPB_UNROLL
+  for (int i = 0; i < NM; ++i) r.m[i] = D[W - NM + i];
+  const uint32_t g = D[W - NM - 1];
+  st |= g << 1;
+  MPB_UNROLL
+  for (int i = 0; i < W - NM - 1; ++i) st |= D[i];
+  int32_t e = ea + (int32_t)cs - (int32_t)(32u * lq + lr);
+  rndn<NM>(r.m, e, g >> 31, st);
+  r.e = e;
+  r.s = s;
+  if (zero) set_zero(r);
+}
+
+/* r = round(x + y), r = round(x - y) */
+template <int N, bool kVote = false>
+MPB_HD void add(fval<N> &r, const fval<N> &x, const fval<N> &y) {
+  add_round<N, N, kVote>(r, x.m, x.e, x.s, y.m, y.e, y.s);
+}
+template <int N, bool kVote = false>
+MPB_HD void sub(fval<N> &r, const fval<N> &x, const fval<N> &y) {
+  add_round<N, N, kVote>(r, x.m, x.e, x.s, y.m, y.e, y.s ^ (is_zero(y) ? 0u : 1u));
+}
+
+/* r = round(a*b + c), one rounding (MPFR mpfr_fma semantics) */
+template <int N, bool kVote = false>
+MPB_HD void fma(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c) {
+  uint32_t p[2 * N], cw[2 * N];
+  int32_t pe;
+  mul_exact_norm<N>(p, pe, a, b);
+  MPB_UNROLL
+  for (int i = 0; i < N; ++i) {
+    cw[i] = 0u;
+    cw[N + i] = c.m[i];
+  }
+  add_round<2 * N, N, kVote>(r, p, pe, a.s ^ b.s, cw, c.e, c.s);
+}
+
+/* round(a*b - c*d) and round(a*b + c*d), one rounding each (MPFR
+ * mpfr_fmms / mpfr_fmma semantics; the exact-intermediate complex product
+ * of MPC_RNDNN, mpc_cuda cu_fcomplex.cuh:91-96) */
+template <int N, bool kVote = false>
+MPB_HD void fmms(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c,
+                 const fval<N> &d, uint32_t negate_cd = 1u) {
+  uint32_t p1[2 * N], p2[2 * N];
+  int32_t e1, e2;
+  mul_exact_norm<N>(p1, e1, a, b);
+  mul_exact_norm<N>(p2, e2, c, d);
+  uint32_t s2 = c.s ^ d.s ^ negate_cd;
+  add_round<2 * N, N, kVote>(r, p1, e1, a.s ^ b.s, p2, e2, s2);
+}
+template <int N, bool kVote = false>
+MPB_HD void fmma(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c,
+                 const fval<N> &d) {
+  fmms<N, kVote>(r, a, b, c, d, 0u);
+}
+
+/* complex (MPC_RNDNN): re = round(ar*br - ai*bi), im = round(ar*bi + ai*br) */
+template <int N, bool kVote = false>
+MPB_HD void cmul(fval<N> &rr, fval<N> &ri, const fval<N> &ar, const fval<N> &ai,
+                 const fval<N> &br, const fval<N> &bi) {
+  fmms<N, kVote>(rr, ar, br, ai, bi, 1u);
+  fmms<N, kVote>(ri, ar, bi, ai, br, 0u);
+}
+
+/* magnitude / signed compare (-1, 0, 1) */
+template <int N>
+MPB_HD int cmpmag(const fval<N> &a, const fval<N> &b) {
+  if (a.e != b.e) return a.e > b.e ? 1 : -1;
+  for (int i = N - 1; i >= 0; --i)
+    if (a.m[i] != b.m[i]) return a.m[i] > b.m[i] ? 1 : -1;
+  return 0;
+}
+
+/* ------------------------------------------------------------------ *
+ * head word of the in-memory format: (e << 1) | s, zero = 0x80000000
+ * ------------------------------------------------------------------ */
+MPB_HD uint32_t pack_head(int32_t e, uint32_t s) { return ((uint32_t)e << 1) | s; }
+MPB_HD int32_t head_exp(uint32_t h) { return (int32_t)h >> 1; }
+MPB_HD uint32_t head_sign(uint32_t h) { return h & 1u; }
+constexpr uint32_t kHeadZero = 0x80000000u;
+
+} /* namespace mpb */
+
+#endif /* MPB_CORE_CUH */

@@ -1,0 +1,209 @@
+"""mpc_cuda_b200 -- Python host side of the mpb B200 fixed-precision engine.
+
+The engine is ``libmpb.so`` (CUDA, sm_100a) behind the C ABI of
+``include/mpb.h``.  This module binds that ABI with ctypes and accepts torch
+CUDA tensors (any dtype; the bytes are used) as device buffers; torch supplies
+device memory and streams only.  There is no CPU implementation: if the
+library is missing or no GPU is present every compute call raises.
+
+Buffers hold the tiled layout (``mpc_cuda_b200.layout``):
+``vec_bytes(prec, n)`` bytes for a real vector, ``cvec_bytes`` for complex,
+row-major matrices with a leading dimension that is a multiple of 32.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+from . import layout
+from .layout import SUPPORTED, aos_bytes, tile_bytes
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmpb.so")
+HOST_LIB_PATH = os.path.join(HERE, "libmpb_host.so")
+
+MPB_OP_MUL, MPB_OP_ADD, MPB_OP_SUB = 0, 1, 2
+
+_STATUS = {
+    0: "MPB_OK", -1: "MPB_ERR_PREC", -2: "MPB_ERR_SIZE", -3: "MPB_ERR_NULL", -4: "MPB_ERR_ALIGN",
+    -5: "MPB_ERR_LD", -6: "MPB_ERR_CUDA", -7: "MPB_ERR_ARG", -8: "MPB_ERR_WORKSPACE",
+}
+
+
+class MpbError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        super().__init__(f"{where}: {_STATUS.get(status, status)} ({status_string(status)})")
+
+
+_lib = None
+_host = None
+
+# name -> argument types (after the leading int prec where present)
+_V, _S, _I, _L = C.c_void_p, C.c_size_t, C.c_int, C.c_long
+_SIGS = {
+    "mpb_version": ([], C.c_int),
+    "mpb_status_string": ([_I], C.c_char_p),
+    "mpb_prec_supported": ([_I], C.c_int),
+    "mpb_vec_bytes": ([_I, _S], C.c_size_t),
+    "mpb_cvec_bytes": ([_I, _S], C.c_size_t),
+    "mpb_aos_bytes": ([_I], C.c_size_t),
+    "mpb_pack_aos": ([_I, _S, _V, _V, _V], C.c_int),
+    "mpb_unpack_aos": ([_I, _S, _V, _V, _V], C.c_int),
+    "mpb_cpack_aos": ([_I, _S, _V, _V, _V], C.c_int),
+    "mpb_cunpack_aos": ([_I, _S, _V, _V, _V], C.c_int),
+    "mpb_from_double": ([_I, _S, _V, _V, _V], C.c_int),
+    "mpb_to_double": ([_I, _S, _V, _V, _V], C.c_int),
+    "mpb_binop_r": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
+    "mpb_fma_r": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
+    "mpb_binop_c": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
+    "mpb_axpy_r": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
+    "mpb_axpy_c": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
+    "mpb_gemv_r": ([_I, _S, _S, _V, _S, _V, _V, _V, _V], C.c_int),
+    "mpb_gemv_c": ([_I, _S, _S, _V, _S, _V, _V, _V, _V], C.c_int),
+    "mpb_gemm_r": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _V], C.c_int),
+    "mpb_gemm_c": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _V], C.c_int),
+}
+
+
+def build(verbose: bool = False) -> None:
+    """Compile libmpb.so / libmpb_host.so in-tree (nvcc, sm_100a)."""
+    out = subprocess.run(["make", "-C", os.path.join(HERE, "csrc"), "-j8"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("mpb build failed:\n" + out.stdout[-4000:] + out.stderr[-4000:])
+    if verbose:
+        print(out.stdout)
+
+
+def lib():
+    """The loaded CUDA engine.  Raises if libmpb.so was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run mpc_cuda_b200.build() (nvcc, sm_100a)")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def host_lib():
+    """The drop-in cu_fp surface built for the host CPU (AoS arrays)."""
+    global _host
+    if _host is None:
+        if not os.path.exists(HOST_LIB_PATH):
+            raise RuntimeError(f"{HOST_LIB_PATH} is missing: run mpc_cuda_b200.build()")
+        H = C.CDLL(HOST_LIB_PATH)
+        for name in ("mpbh_binop", "mpbh_cbinop"):
+            getattr(H, name).argtypes = [_I, _I, _L, _V, _V, _V]
+        H.mpbh_fma.argtypes = [_I, _L, _V, _V, _V, _V]
+        for name in ("mpbh_axpy_r", "mpbh_axpy_c"):
+            getattr(H, name).argtypes = [_I, _L, _V, _V, _V, _V]
+        H.mpbh_from_double.argtypes = [_I, _L, _V, _V]
+        H.mpbh_to_double.argtypes = [_I, _L, _V, _V]
+        _host = H
+    return _host
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+def status_string(status: int) -> str:
+    try:
+        return lib().mpb_status_string(status).decode()
+    except Exception:  # library missing: still describe the code
+        return _STATUS.get(status, "unknown")
+
+
+def vec_bytes(prec: int, n: int, cplx: bool = False) -> int:
+    return layout.vec_bytes(prec, n, cplx)
+
+
+# ---------------------------------------------------------------- buffers
+def _ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def empty(prec: int, n: int, cplx: bool = False, device="cuda"):
+    """Uninitialised device vector of n elements (torch uint8 tensor)."""
+    import torch
+
+    return torch.empty(max(vec_bytes(prec, n, cplx), 16), dtype=torch.uint8, device=device)
+
+
+def empty_matrix(prec: int, rows: int, ld: int, cplx: bool = False, device="cuda"):
+    return empty(prec, rows * ld, cplx, device)
+
+
+def _call(name, *args):
+    rc = getattr(lib(), name)(*args)
+    if rc != 0:
+        raise MpbError(rc, name)
+
+
+# ---------------------------------------------------------------- operations
+def pack_aos(prec, n, aos, vec, cplx=False, stream=None):
+    _call("mpb_cpack_aos" if cplx else "mpb_pack_aos", prec, n, _ptr(aos), _ptr(vec), _stream(stream))
+
+
+def unpack_aos(prec, n, vec, aos, cplx=False, stream=None):
+    _call("mpb_cunpack_aos" if cplx else "mpb_unpack_aos", prec, n, _ptr(vec), _ptr(aos), _stream(stream))
+
+
+def from_double(prec, n, d, vec, stream=None):
+    _call("mpb_from_double", prec, n, _ptr(d), _ptr(vec), _stream(stream))
+
+
+def to_double(prec, n, vec, d, stream=None):
+    _call("mpb_to_double", prec, n, _ptr(vec), _ptr(d), _stream(stream))
+
+
+def binop(prec, op, n, a, b, r, cplx=False, stream=None):
+    _call("mpb_binop_c" if cplx else "mpb_binop_r", prec, op, n, _ptr(a), _ptr(b), _ptr(r), _stream(stream))
+
+
+def fma(prec, n, a, b, c, r, stream=None):
+    _call("mpb_fma_r", prec, n, _ptr(a), _ptr(b), _ptr(c), _ptr(r), _stream(stream))
+
+
+def axpy(prec, n, a, x, y, z, cplx=False, stream=None):
+    """z = a*x + y (a: element 0 of a vector), one rounding per operation."""
+    _call("mpb_axpy_c" if cplx else "mpb_axpy_r", prec, n, _ptr(a), _ptr(x), _ptr(y), _ptr(z), _stream(stream))
+
+
+def gemv(prec, m, n, A, lda, x, y, y_out, cplx=False, stream=None):
+    """y_out = A.x + y, sequential-k per-operation rounding, then + y."""
+    _call("mpb_gemv_c" if cplx else "mpb_gemv_r", prec, m, n, _ptr(A), lda, _ptr(x), _ptr(y), _ptr(y_out),
+          _stream(stream))
+
+
+def gemm(prec, m, n, k, A, lda, B, ldb, Cm, ldc, cplx=False, stream=None):
+    """C = A.B, sequential-k per-operation rounding (plain kernel)."""
+    _call("mpb_gemm_c" if cplx else "mpb_gemm_r", prec, m, n, k, _ptr(A), lda, _ptr(B), ldb, _ptr(Cm), ldc,
+          _stream(stream))
+
+
+__all__ = [
+    "SUPPORTED", "MpbError", "aos_bytes", "tile_bytes", "vec_bytes", "build", "lib", "host_lib", "empty",
+    "empty_matrix", "pack_aos", "unpack_aos", "from_double", "to_double", "binop", "fma", "axpy", "gemv", "gemm",
+    "layout", "MPB_OP_MUL", "MPB_OP_ADD", "MPB_OP_SUB",
+]

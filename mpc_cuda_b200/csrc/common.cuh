@@ -1,0 +1,87 @@
+/* common.cuh -- shared host-side plumbing of the mpb C ABI: precision dispatch,
+ * argument validation, grid sizing.  Internal header (not installed). */
+#ifndef MPB_COMMON_CUH
+#define MPB_COMMON_CUH
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "mpb.h"
+#include "mpb/layout.cuh"
+
+namespace mpb {
+
+/* largest element count any entry point accepts (2^40) */
+constexpr size_t kMaxElems = (size_t)1 << 40;
+
+inline bool prec_ok(int prec) {
+  return prec == 64 || prec == 128 || prec == 256 || prec == 512 || prec == 1024 || prec == 2048;
+}
+inline bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+inline cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
+
+/* a device buffer argument: required when count > 0 */
+inline int check_buf(const void *p) {
+  if (!p) return MPB_ERR_NULL;
+  if (!aligned16(p)) return MPB_ERR_ALIGN;
+  return MPB_OK;
+}
+
+inline int launch_status() {
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MPB_OK : MPB_ERR_CUDA;
+}
+
+/* SM count of the current device (cached per device) */
+int sm_count();
+
+/* Grid for a grid-stride kernel over `work` warp-sized units of 32 threads
+ * each: enough blocks to fill every SM at the kernel's occupancy, never more
+ * than the work needs. */
+template <typename K>
+inline int grid_for(K kernel, int block, size_t threads_needed) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const size_t full = (size_t)sm_count() * (size_t)per_sm;
+  const size_t need = (threads_needed + (size_t)block - 1) / (size_t)block;
+  size_t g = need < full ? need : full;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+} /* namespace mpb */
+
+/* runtime precision -> compile-time limb count N (32-bit limbs) */
+#define MPB_DISPATCH_PREC(prec, ...)            \
+  switch (prec) {                               \
+    case 64: {                                  \
+      constexpr int N = 2;                      \
+      __VA_ARGS__;                              \
+    } break;                                    \
+    case 128: {                                 \
+      constexpr int N = 4;                      \
+      __VA_ARGS__;                              \
+    } break;                                    \
+    case 256: {                                 \
+      constexpr int N = 8;                      \
+      __VA_ARGS__;                              \
+    } break;                                    \
+    case 512: {                                 \
+      constexpr int N = 16;                     \
+      __VA_ARGS__;                              \
+    } break;                                    \
+    case 1024: {                                \
+      constexpr int N = 32;                     \
+      __VA_ARGS__;                              \
+    } break;                                    \
+    case 2048: {                                \
+      constexpr int N = 64;                     \
+      __VA_ARGS__;                              \
+    } break;                                    \
+    default:                                    \
+      return MPB_ERR_PREC;                      \
+  }
+
+#endif /* MPB_COMMON_CUH */

@@ -121,7 +121,7 @@ def empty(prec: int, n: int, cplx: bool = False) -> np.ndarray:
 
 def gen_pairs(prec: int, n: int, seed: int, cplx: bool = False):
     """The reference's seeded random operand pairs (tools/test_freal.cu:55,
-    tools/test_fcomplex.cu:160-162): xorshift64 stream, exponent spread 40 for
+    tools/test_fcomplex.cu:55-57): xorshift64 stream, exponent spread 40 for
     three of every four pairs and PB+200 for the fourth."""
     A, B = empty(prec, n, cplx), empty(prec, n, cplx)
     f = lib().orc_gen_pairs_c if cplx else lib().orc_gen_pairs_r

@@ -17,7 +17,7 @@
  *  (2) The same operations computed by the system MPFR 4.2.1 / MPC 1.3.1
  *      libraries (through mpfr_shim.h), which is the correctness oracle the
  *      reference itself is tested against (tools/test_freal.cu:69-76,
- *      tools/test_fcomplex.cu:176-183, tools/linalg_fast.cu:71-83).
+ *      tools/test_fcomplex.cu:71-78, tools/linalg_fast.cu:71-83).
  *
  * Element format (both halves): the reference's AoS struct cu_freal<PB>
  *   { int32 sign; int32 pad; int64 exp; uint64 m[N64]; }   N64 = ceil(PB/64)
@@ -867,7 +867,7 @@ u64 orc_gen_pairs_r(int P, long M, u64 seed, void *A, void *B) {
   }
   return seed;
 }
-/* complex pairs: A.re, A.im, B.re, B.im in that order (tools/test_fcomplex.cu:160-162) */
+/* complex pairs: A.re, A.im, B.re, B.im in that order (tools/test_fcomplex.cu:55-57) */
 u64 orc_gen_pairs_c(int P, long M, u64 seed, void *A, void *B) {
   size_t e1 = esz_of(P), es = 2 * e1;
   for (long i = 0; i < M; i++) {

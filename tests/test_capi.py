@@ -1,0 +1,69 @@
+"""The C ABI library: loads without a GPU, exports every symbol mpb.h declares,
+and rejects bad arguments on the host with the documented status codes
+(no kernel is launched by any call here)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            src = open(os.path.join(ROOT, "include", fn)).read()
+            names |= set(re.findall(r"\b(mpb_[a-z0-9_]+)\s*\(", src))
+    return sorted(names)
+
+
+def test_exports_every_declared_symbol(mpb):
+    lib = C.CDLL(mpb.LIB_PATH)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, f"declared but not exported: {missing}"
+    assert set(declared_symbols()) <= set(mpb.exported_symbols())
+
+
+def test_info_calls(mpb):
+    L = mpb.lib()
+    assert L.mpb_version() >= 100
+    for p in (64, 128, 256, 512, 1024, 2048):
+        assert L.mpb_prec_supported(p) == 1
+        assert L.mpb_vec_bytes(p, 33) == mpb.vec_bytes(p, 33)
+        assert L.mpb_cvec_bytes(p, 33) == mpb.vec_bytes(p, 33, True)
+        assert L.mpb_aos_bytes(p) == 16 + p // 8
+    for p in (0, 32, 96, 100, 4096, -64):
+        assert L.mpb_prec_supported(p) == 0
+        assert L.mpb_vec_bytes(p, 10) == 0
+    assert b"precision" in L.mpb_status_string(-1)
+
+
+def test_bad_arguments_rejected_on_host(mpb):
+    L = mpb.lib()
+    good = 4096  # a fake, 16-byte aligned "device" address: never dereferenced here
+    # unsupported precision
+    assert L.mpb_axpy_r(96, 10, good, good, good, good, None) == -1
+    assert L.mpb_gemm_r(100, 4, 4, 4, good, 32, good, 32, good, 32, None) == -1
+    # null and misaligned buffers
+    assert L.mpb_axpy_r(256, 10, None, good, good, good, None) == -3
+    assert L.mpb_axpy_c(256, 10, good, good, good + 8, good, None) == -4
+    assert L.mpb_binop_r(256, 0, 10, good, None, good, None) == -3
+    # bad op code
+    assert L.mpb_binop_r(256, 7, 10, good, good, good, None) == -7
+    # leading dimensions: not a multiple of 32, or shorter than a row
+    assert L.mpb_gemm_r(256, 4, 4, 4, good, 33, good, 32, good, 32, None) == -5
+    assert L.mpb_gemm_r(256, 4, 40, 4, good, 32, good, 32, good, 32, None) == -5
+    assert L.mpb_gemv_r(256, 4, 50, good, 32, good, good, good, None) == -5
+    # size overflow
+    assert L.mpb_axpy_r(256, 1 << 62, good, good, good, good, None) == -2
+
+
+def test_empty_inputs_are_noops(mpb):
+    L = mpb.lib()
+    assert L.mpb_axpy_r(256, 0, None, None, None, None, None) == 0
+    assert L.mpb_axpy_c(1024, 0, None, None, None, None, None) == 0
+    assert L.mpb_gemm_r(512, 0, 8, 8, None, 32, None, 32, None, 32, None) == 0
+    assert L.mpb_gemv_c(256, 0, 5, None, 32, None, None, None, None) == 0
+    assert L.mpb_pack_aos(256, 0, None, None, None) == 0

@@ -1,0 +1,205 @@
+"""GPU parity: every engine entry point, called through the C ABI, against the
+CPU oracle -- bit for bit (integer arithmetic: no tolerance).
+
+Operands follow the reference's test method (seeded xorshift pairs with
+exponent spreads 40 / PB+200, tools/test_freal.cu:17-27,55) and the
+benchmark workloads' value distributions; expected results come from the
+system MPFR/MPC (``mp_*``) or the oracle's restatement (``orc_*``), which
+tests/test_oracle.py pins to each other and to the reference headers.
+"""
+import numpy as np
+import pytest
+
+from conftest import to_dev, to_host
+from mpc_cuda_b200 import layout, synth
+
+pytestmark = pytest.mark.gpu
+PRECS = layout.SUPPORTED
+
+
+def dvec(prec, aos, cplx=False):
+    return to_dev(layout.aos_to_vec(prec, aos, cplx))
+
+
+def hvec(prec, t, n, cplx=False):
+    return layout.vec_to_aos(prec, to_host(t), n, cplx)
+
+
+def zero_aos(prec, n, cplx=False):
+    z = np.zeros((n, layout.aos_bytes(prec)), np.uint8)
+    z[:, 0:4] = np.array([1], np.int32).view(np.uint8)
+    z[:, 8:16] = np.array([layout.AOS_ZERO_EXP], np.int64).view(np.uint8)
+    return np.concatenate([z, z], axis=1) if cplx else z
+
+
+def pad_rows(prec, A, rows, cols, ld, cplx=False):
+    """AoS rows x cols -> AoS rows x ld with zero elements in the padding."""
+    es = A.shape[1]
+    out = np.repeat(zero_aos(prec, 1, cplx), rows * ld, axis=0).reshape(rows, ld, es)
+    out[:, :cols] = A.reshape(rows, cols, es)
+    return out.reshape(rows * ld, es)
+
+
+def unpad_rows(A, rows, cols, ld):
+    es = A.shape[1]
+    return A.reshape(rows, ld, es)[:, :cols].reshape(rows * cols, es)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_binops_real(orc, mpb, prec):
+    M = 100000 if prec <= 1024 else 30000  # 100k pairs as in tools/test_freal.cu:89
+    A, B = orc.gen_pairs(prec, M, 0xBEEF + prec)
+    a, b, r = dvec(prec, A), dvec(prec, B), mpb.empty(prec, M)
+    for op, kind in enumerate(("mul", "add", "sub")):
+        mpb.binop(prec, op, M, a, b, r)
+        bad, first = orc.mismatches(prec, hvec(prec, r, M), orc.binop(kind, prec, A, B, "mp"))
+        assert bad == 0, f"{kind} PB={prec}: {bad} mismatches, first at {first}"
+    Cc, _ = orc.gen_pairs(prec, M, 0xFACE + prec)
+    mpb.fma(prec, M, a, b, dvec(prec, Cc), r)
+    bad, first = orc.mismatches(prec, hvec(prec, r, M), orc.fma(prec, A, B, Cc, "mp"))
+    assert bad == 0, f"fma PB={prec}: {bad} mismatches, first at {first}"
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_binops_complex(orc, mpb, prec):
+    M = 30000 if prec <= 1024 else 6000
+    A, B = orc.gen_pairs(prec, M, 0xC0DE + prec, cplx=True)
+    a, b, r = dvec(prec, A, True), dvec(prec, B, True), mpb.empty(prec, M, True)
+    for op, kind in enumerate(("cmul", "cadd", "csub")):
+        mpb.binop(prec, op, M, a, b, r, cplx=True)
+        bad, first = orc.mismatches(prec, hvec(prec, r, M, True), orc.binop(kind, prec, A, B, "mp"), True)
+        assert bad == 0, f"{kind} PB={prec}: {bad} mismatches, first at {first}"
+
+
+@pytest.mark.parametrize("cplx", (False, True))
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("n", (1, 31, 33, 1000))
+def test_pack_unpack_and_ragged_sizes(orc, mpb, prec, n, cplx):
+    import torch
+
+    A, _ = orc.gen_pairs(prec, n, 0x51 + n, cplx)
+    aos = torch.from_numpy(A.reshape(-1).copy()).cuda()
+    v = mpb.empty(prec, n, cplx)
+    mpb.pack_aos(prec, n, aos, v, cplx)
+    assert np.array_equal(to_host(v)[: layout.vec_bytes(prec, n, cplx)], layout.aos_to_vec(prec, A, cplx))
+    back = torch.zeros_like(aos)
+    mpb.unpack_aos(prec, n, v, back, cplx)
+    assert np.array_equal(to_host(back).reshape(A.shape), A)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_double_conversions(orc, mpb, prec):
+    import torch
+
+    rng = np.random.default_rng(prec)
+    d = np.concatenate([rng.uniform(-1, 1, 5000), [0.0, 1.5, -1e-300, 3e300, 2.0**-1022]])
+    n = d.size
+    td = torch.from_numpy(d).cuda()
+    v = mpb.empty(prec, n)
+    mpb.from_double(prec, n, td, v)
+    ref = orc.empty(prec, n)
+    orc.lib().orc_from_double(prec, n, d.ctypes.data, ref.ctypes.data)
+    assert orc.mismatches(prec, hvec(prec, v, n), ref)[0] == 0
+    # to_double of random full-width values (overflow/underflow included):
+    # same rounding as the host build of the drop-in surface and the reference
+    A, _ = orc.gen_pairs(prec, 4000, 3 + prec)
+    out = torch.zeros(4000, dtype=torch.float64, device="cuda")
+    mpb.to_double(prec, 4000, dvec(prec, A), out)
+    exp = np.zeros(4000)
+    mpb.host_lib().mpbh_to_double(prec, 4000, A.ctypes.data, exp.ctypes.data)
+    assert np.array_equal(out.cpu().numpy(), exp)
+    if orc.ref_available():
+        exp2 = np.zeros(4000)
+        orc.ref().ref_to_double(prec, 4000, A.ctypes.data, exp2.ctypes.data)
+        assert np.array_equal(exp, exp2)
+
+
+@pytest.mark.parametrize("cplx", (False, True))
+@pytest.mark.parametrize("prec", PRECS)
+def test_axpy_reference_pairs(orc, mpb, prec, cplx):
+    n = 20000 if prec <= 1024 else 4000
+    X, Y = orc.gen_pairs(prec, n, 0xA0 + prec, cplx)
+    a = X[7:8].copy()
+    z = mpb.empty(prec, n, cplx)
+    mpb.axpy(prec, n, dvec(prec, a, cplx), dvec(prec, X, cplx), dvec(prec, Y, cplx), z, cplx)
+    bad, first = orc.mismatches(prec, hvec(prec, z, n, cplx), orc.axpy(prec, a, X, Y, cplx, impl="mp"), cplx)
+    assert bad == 0, f"axpy PB={prec} cplx={cplx}: first mismatch {first}"
+
+
+def test_axpy_real_pb256_full_size(orc, mpb):
+    """The real AXPY workload at full size (PB=256, n=2^20, a=1.5, FP64 inputs)."""
+    prec, n = 256, 1 << 20
+    a, x, y = synth.axpy_r256(n=n)
+    A, X, Y = (layout.aos_from_parts(prec, *p) for p in (a, x, y))
+    z = mpb.empty(prec, n)
+    mpb.axpy(prec, n, to_dev(layout.vec_from_parts(prec, *a)), to_dev(layout.vec_from_parts(prec, *x)),
+             to_dev(layout.vec_from_parts(prec, *y)), z)
+    bad, first = orc.mismatches(prec, hvec(prec, z, n), orc.axpy(prec, A, X, Y))
+    assert bad == 0, f"first mismatch {first}"
+
+
+def test_axpy_complex_pb1024_full_size(orc, mpb):
+    """The complex AXPY workload at full size (PB=1024, n=2^18, 1% zeros)."""
+    prec, n = 1024, 1 << 18
+    a, x, y = synth.axpy_c1024(n=n)
+    A, X, Y = (synth.interleave_complex(prec, *p) for p in (a, x, y))
+    z = mpb.empty(prec, n, True)
+    mpb.axpy(prec, n, dvec(prec, A, True), dvec(prec, X, True), dvec(prec, Y, True), z, cplx=True)
+    bad, first = orc.mismatches(prec, hvec(prec, z, n, True), orc.axpy(prec, A, X, Y, True), True)
+    assert bad == 0, f"first mismatch {first}"
+
+
+@pytest.mark.parametrize("cplx", (False, True))
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("shape", ((1, 1, 1), (5, 7, 33), (33, 40, 17), (64, 64, 64)))
+def test_gemm_plain(orc, mpb, prec, shape, cplx):
+    m, n, k = shape
+    if prec == 2048 and m * n * k > 40000:
+        pytest.skip("covered at smaller shapes")
+    A, _ = orc.gen_pairs(prec, m * k, 0x61 + m + prec, cplx)
+    B, _ = orc.gen_pairs(prec, k * n, 0x62 + n + prec, cplx)
+    lda, ldb, ldc = (-(-k // 32) * 32, -(-n // 32) * 32, -(-n // 32) * 32)
+    Cd = mpb.empty(prec, m * ldc, cplx)
+    mpb.gemm(prec, m, n, k, dvec(prec, pad_rows(prec, A, m, k, lda, cplx), cplx), lda,
+             dvec(prec, pad_rows(prec, B, k, n, ldb, cplx), cplx), ldb, Cd, ldc, cplx)
+    got = unpad_rows(hvec(prec, Cd, m * ldc, cplx), m, n, ldc)
+    exp = orc.gemm(prec, m, n, k, A, k, B, n, cplx, impl="mp")
+    bad, first = orc.mismatches(prec, got, exp, cplx)
+    assert bad == 0, f"gemm PB={prec} {shape}: first mismatch {first}"
+
+
+@pytest.mark.parametrize("cplx", (False, True))
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("shape", ((1, 1), (16, 17), (37, 70), (130, 33)))
+def test_gemv_plain(orc, mpb, prec, shape, cplx):
+    m, n = shape
+    A, _ = orc.gen_pairs(prec, m * n, 0x71 + m + prec, cplx)
+    x, _ = orc.gen_pairs(prec, n, 0x72 + n, cplx)
+    y, _ = orc.gen_pairs(prec, m, 0x73 + m, cplx)
+    lda = -(-n // 32) * 32
+    yo = mpb.empty(prec, m, cplx)
+    mpb.gemv(prec, m, n, dvec(prec, pad_rows(prec, A, m, n, lda, cplx), cplx), lda, dvec(prec, x, cplx),
+             dvec(prec, y, cplx), yo, cplx)
+    exp = orc.gemv(prec, m, n, A, n, x, y, cplx, impl="mp")
+    bad, first = orc.mismatches(prec, hvec(prec, yo, m, cplx), exp, cplx)
+    assert bad == 0, f"gemv PB={prec} {shape}: first mismatch {first}"
+
+
+def test_gemm_real_pb512_rows_sample(orc, mpb):
+    """The 1024^3 PB=512 matmul workload at full size; a row sample is checked
+    against the oracle (the whole product is ~1e9 MPFR multiply-adds)."""
+    prec, m, n, k = 512, 1024, 1024, 1024
+    (al, ah), (bl, bh) = synth.gemm_r512()
+    Cd = mpb.empty(prec, m * n)
+    mpb.gemm(prec, m, n, k, to_dev(layout.vec_from_parts(prec, al, ah)), k,
+             to_dev(layout.vec_from_parts(prec, bl, bh)), n, Cd, n)
+    got = hvec(prec, Cd, m * n)
+    A, B = layout.aos_from_parts(prec, al, ah), layout.aos_from_parts(prec, bl, bh)
+    rows = (0, 4)
+    exp = orc.gemm(prec, m, n, k, A, k, B, n, rows=rows)
+    es = got.shape[1]
+    sel = slice(rows[0] * n, rows[1] * n)
+    assert orc.mismatches(prec, got[sel], exp[sel])[0] == 0
+    last = orc.gemm(prec, m, n, k, A, k, B, n, rows=(m - 2, m))
+    assert orc.mismatches(prec, got[(m - 2) * n:], last[(m - 2) * n:])[0] == 0
+    assert es == layout.aos_bytes(prec)

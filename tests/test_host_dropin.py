@@ -1,0 +1,87 @@
+"""The drop-in cu_fp surface, built for the host CPU, against MPFR/MPC.
+
+This exercises the exact code the device runs (the mpb core), with each PTX
+carry-chain instruction emulated on the host, on the reference's own test
+method: seeded xorshift operand pairs (tools/test_freal.cu:17-27,55),
+precisions including the sub-limb SB=32 cases (96, 160, 288, 1056), and
+equality in mpfr_equal_p / mpc_cmp semantics.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+PRECS = (32, 64, 96, 128, 160, 256, 288, 512, 1024, 1056, 2048)
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_real_ops(orc, mpb, prec):
+    H = mpb.host_lib()
+    M = 12000 if prec <= 1056 else 3000
+    A, B = orc.gen_pairs(prec, M, 0x1111 * (prec // 32))
+    for op, kind in enumerate(("mul", "add", "sub")):
+        R = orc.empty(prec, M)
+        assert H.mpbh_binop(prec, op, M, _p(A), _p(B), _p(R)) == 0
+        bad, first = orc.mismatches(prec, R, orc.binop(kind, prec, A, B, "mp"))
+        assert bad == 0, f"{kind} PB={prec}: first mismatch {first}"
+    Cc, _ = orc.gen_pairs(prec, M, 0x77 + prec)
+    R = orc.empty(prec, M)
+    assert H.mpbh_fma(prec, M, _p(A), _p(B), _p(Cc), _p(R)) == 0
+    assert orc.mismatches(prec, R, orc.fma(prec, A, B, Cc, "mp"))[0] == 0
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_complex_ops(orc, mpb, prec):
+    H = mpb.host_lib()
+    M = 3000 if prec <= 1056 else 800
+    A, B = orc.gen_pairs(prec, M, 0x11 * (prec // 32), cplx=True)
+    for op, kind in enumerate(("cmul", "cadd", "csub")):
+        R = orc.empty(prec, M, True)
+        assert H.mpbh_cbinop(prec, op, M, _p(A), _p(B), _p(R)) == 0
+        bad, first = orc.mismatches(prec, R, orc.binop(kind, prec, A, B, "mp"), True)
+        assert bad == 0, f"{kind} PB={prec}: first mismatch {first}"
+
+
+@pytest.mark.parametrize("cplx", (False, True))
+@pytest.mark.parametrize("prec", (64, 256, 1024))
+def test_axpy_host(orc, mpb, prec, cplx):
+    H = mpb.host_lib()
+    X, Y = orc.gen_pairs(prec, 2000, 0x99 + prec, cplx)
+    a = X[:1].copy()
+    Z = orc.empty(prec, 2000, cplx)
+    f = H.mpbh_axpy_c if cplx else H.mpbh_axpy_r
+    assert f(prec, 2000, _p(a), _p(X), _p(Y), _p(Z)) == 0
+    assert orc.mismatches(prec, Z, orc.axpy(prec, a, X, Y, cplx, impl="mp"), cplx)[0] == 0
+
+
+def test_sample_fixed_known_values(mpb):
+    """Known values printed by the reference's sample (demos/sample_fixed.cu:59-67):
+    1.5*(1/3)+1.5 and (1.5-0.25i)*(1+0.5i)+(2-1i) at 256 bits."""
+    H = mpb.host_lib()
+    prec = 256
+    es = 16 + prec // 8
+    d = np.array([1.5, 1.0 / 3.0], dtype=np.float64)
+    v = np.zeros((2, es), dtype=np.uint8)
+    assert H.mpbh_from_double(prec, 2, _p(d), _p(v)) == 0
+    t = np.zeros((1, es), dtype=np.uint8)
+    r = np.zeros((1, es), dtype=np.uint8)
+    H.mpbh_binop(prec, 0, 1, _p(v[0:1].copy()), _p(v[1:2].copy()), _p(t))
+    H.mpbh_binop(prec, 1, 1, _p(t), _p(v[0:1].copy()), _p(r))
+    out = np.zeros(1)
+    H.mpbh_to_double(prec, 1, _p(r), _p(out))
+    assert out[0] == 1.5 * (1.0 / 3.0) + 1.5
+    zd = np.array([1.5, -0.25, 1.0, 0.5, 2.0, -1.0])
+    zz = np.zeros((6, es), dtype=np.uint8)
+    H.mpbh_from_double(prec, 6, _p(zd), _p(zz))
+    za, zx, zy = (zz[0:2].reshape(1, -1).copy(), zz[2:4].reshape(1, -1).copy(), zz[4:6].reshape(1, -1).copy())
+    t = np.zeros((1, 2 * es), dtype=np.uint8)
+    r = np.zeros((1, 2 * es), dtype=np.uint8)
+    H.mpbh_cbinop(prec, 0, 1, _p(za), _p(zx), _p(t))
+    H.mpbh_cbinop(prec, 1, 1, _p(t), _p(zy), _p(r))
+    out = np.zeros(2)
+    H.mpbh_to_double(prec, 2, _p(r.reshape(2, es).copy()), _p(out))
+    assert tuple(out) == (3.625, -0.5)
