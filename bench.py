@@ -66,7 +66,7 @@ class Clocks:
             self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "20"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
@@ -189,6 +189,10 @@ class AxpyWorkload:
     def units(self):
         return self.n
 
+    @property
+    def default_steps(self):
+        return 4000 if self.cplx else 40000
+
     def step(self, i, stream):
         x, y, z = self.sets[i % self.nsets]
         self.M.axpy(self.prec, self.n, self.a, x, y, z, self.cplx, stream=stream)
@@ -232,10 +236,14 @@ class AxpyWorkload:
                 "traffic": None, "hbm": hbm}
 
     def cpu_run(self, impl, count):
+        """AXPY over the first count elements; returns the units computed."""
         import oracle as O
 
         A, X, Y = self.host
-        return O.axpy(self.prec, A, X[:count], Y[:count], self.cplx, impl=impl)
+        O.axpy(self.prec, A, X[:count], Y[:count], self.cplx, impl=impl)
+        return count
+
+    cpu_probe_units = 2048
 
     def config(self):
         return {"workload": self.desc, "prec": self.prec, "n": self.n,
@@ -245,32 +253,186 @@ class AxpyWorkload:
                 "l2": f"{self.nsets} rotating input sets, {self.nsets * 3 * self.n * self.elem_bytes >> 20} MiB > L2"}
 
 
+def int8_peak_ops(device):
+    """Dense int8 tensor-core throughput of this GPU: cuBLASLt int8 GEMM
+    (torch._int_mm, 8192^3, int32 out), best of 5, ops = 2*M*N*K."""
+    import torch
+
+    try:
+        M = 8192
+        a = torch.randint(-128, 127, (M, M), dtype=torch.int8, device=device)
+        b = torch.randint(-128, 127, (M, M), dtype=torch.int8, device=device).t()
+        torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        return 2.0 * M**3 / (best / 1e3)
+    except Exception:
+        return None
+
+
+class GemmWorkload:
+    """C = A.B, m x n x k at precision prec: the exact-accumulation INT8
+    tensor-core GEMM (one rounding per entry) is the timed step; the plain
+    per-operation-rounded kernel on the same operands is timed beside it."""
+
+    def __init__(self, name, prec, m, n, k, sp_bits, gen):
+        self.name, self.prec, self.m, self.n, self.k, self.sp_bits, self.gen = name, prec, m, n, k, sp_bits, gen
+        self.cplx = False
+        self.S = (prec + sp_bits + 2 + 7) // 8
+        self.desc = (f"real matmul C=A.B, cu_freal<{prec}>, {m}x{n}x{k}: exact-accumulation GEMM on INT8 "
+                     f"tensor cores (one rounding per entry, {self.S} digit slices) vs plain sequential-k kernel")
+
+    @property
+    def default_steps(self):
+        return 20
+
+    launches_per_step = 7  # stats x2, slice x2, tensor-core GEMM, round, fallback
+    e2e_launches_per_step = 10
+
+    def make_host(self, rank):
+        from mpc_cuda_b200 import layout
+
+        (al, ah), (bl, bh) = self.gen(seed=0x5EED3 + 1000 * rank)
+        self.parts = ((al, ah), (bl, bh))
+        return layout.aos_from_parts(self.prec, al, ah), layout.aos_from_parts(self.prec, bl, bh)
+
+    def setup(self, rank, device):
+        import torch
+
+        import mpc_cuda_b200 as M
+        from mpc_cuda_b200 import layout
+
+        self.M = M
+        A, B = self.make_host(rank)
+        self.host = (A, B)
+        (al, ah), (bl, bh) = self.parts
+        self.dA = dev_from(layout.vec_from_parts(self.prec, al, ah), device)
+        self.dB = dev_from(layout.vec_from_parts(self.prec, bl, bh), device)
+        self.dC = M.empty(self.prec, self.m * self.n, device=device)
+        self.dC2 = M.empty(self.prec, self.m * self.n, device=device)
+        self.ws = torch.empty(M.gemm_exact_workspace(self.prec, self.m, self.n, self.k, self.sp_bits),
+                              dtype=torch.uint8, device=device)
+        self.status = torch.zeros(2, dtype=torch.int32, device=device)
+        self.hA, self.hB = pinned_from(A), pinned_from(B)
+        self.hC = torch.empty(self.m * self.n * A.shape[1], dtype=torch.uint8).pin_memory()
+        self.dA_aos = torch.empty(A.size, dtype=torch.uint8, device=device)
+        self.dB_aos = torch.empty(B.size, dtype=torch.uint8, device=device)
+        self.dC_aos = torch.empty(self.hC.numel(), dtype=torch.uint8, device=device)
+        self.eA = M.empty(self.prec, self.m * self.k, device=device)
+        self.eB = M.empty(self.prec, self.k * self.n, device=device)
+
+    def units(self):
+        return self.m * self.n * self.k
+
+    def step(self, i, stream):
+        self.M.gemm_exact(self.prec, self.m, self.n, self.k, self.dA, self.k, self.dB, self.n, self.dC, self.n,
+                          sp_bits=self.sp_bits, workspace=self.ws, status=self.status, stream=stream)
+
+    def e2e_step(self, i, stream):
+        M = self.M
+        self.dA_aos.copy_(self.hA, non_blocking=True)
+        self.dB_aos.copy_(self.hB, non_blocking=True)
+        M.pack_aos(self.prec, self.m * self.k, self.dA_aos, self.eA, stream=stream)
+        M.pack_aos(self.prec, self.k * self.n, self.dB_aos, self.eB, stream=stream)
+        M.gemm_exact(self.prec, self.m, self.n, self.k, self.eA, self.k, self.eB, self.n, self.dC, self.n,
+                     sp_bits=self.sp_bits, workspace=self.ws, status=self.status, stream=stream)
+        M.unpack_aos(self.prec, self.m * self.n, self.dC, self.dC_aos, stream=stream)
+        self.hC.copy_(self.dC_aos, non_blocking=True)
+
+    def e2e_bytes(self):
+        return self.host[0].size + self.host[1].size, self.hC.numel()
+
+    def extra(self, stream, steps=3):
+        """plain kernel rate on the same operands, dominant-kernel time, status"""
+        import torch
+
+        M = self.M
+        M.gemm(self.prec, self.m, self.n, self.k, self.dA, self.k, self.dB, self.n, self.dC2, self.n, stream=stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            M.gemm(self.prec, self.m, self.n, self.k, self.dA, self.k, self.dB, self.n, self.dC2, self.n,
+                   stream=stream)
+        e1.record()
+        torch.cuda.synchronize()
+        plain_ms = e0.elapsed_time(e1) / steps
+        st = self.status.cpu().tolist()
+        return {"plain_ms_per_step": plain_ms, "plain_value": self.units() / (plain_ms / 1e3), "status": st}
+
+    def roofline_tensor(self, tensor_ms, int8_ops):
+        ops = 2.0 * self.units() * self.S * self.S
+        achieved = ops / (tensor_ms / 1e3)
+        return {"bound": "tensor", "achieved": round(achieved / 1e12, 1), "unit": "TOP/s (int8)",
+                "peak": round(int8_ops / 1e12, 1) if int8_ops else None,
+                "frac": round(achieved / int8_ops, 4) if int8_ops else None,
+                "ops_per_unit": 2 * self.S * self.S, "kernel": "k_diag_gemm (tcgen05.mma kind::i8)",
+                "kernel_ms": round(tensor_ms, 4),
+                "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm), measured in this run",
+                "traffic": None}
+
+    def cpu_run(self, impl, count):
+        """The first rows of C on the CPU (sequential-k, per-operation
+        rounding: the reference's matmul); returns the units computed."""
+        import oracle as O
+
+        A, B = self.host
+        rows = max(1, min(self.m, count // (self.n * self.k)))
+        O.gemm(self.prec, self.m, self.n, self.k, A, self.k, B, self.n, impl=impl, rows=(0, rows))
+        return rows * self.n * self.k
+
+    @property
+    def cpu_probe_units(self):
+        return self.n * self.k  # one row of C
+
+    def config(self):
+        return {"workload": self.desc, "prec": self.prec, "m": self.m, "n": self.n, "k": self.k,
+                "sp_bits": self.sp_bits, "slices": self.S,
+                "units": "mp-FMA (one exact product accumulated)",
+                "l2": "operands 143 MB > L2; digit planes 145 MB and diagonal planes 575 MB stream through HBM"}
+
+
 WORKLOADS = {
     "axpy_c1024": lambda: AxpyWorkload("axpy_c1024", True, 1024, 1 << 18, 0x5EED2),
     "axpy_r256": lambda: AxpyWorkload("axpy_r256", False, 256, 1 << 20, 0x5EED1),
+    "gemm_r512": lambda: GemmWorkload("gemm_r512", 512, 1024, 1024, 1024, 32,
+                                      lambda seed: __import__("mpc_cuda_b200.synth", fromlist=["x"]).gemm_r512(seed)),
 }
 DEFAULT_WORKLOAD = "axpy_c1024"
 
 
 # ------------------------------------------------------------------ CPU side
-def cpu_baseline(wl, max_seconds=15.0):
-    """Time the reference's CPU implementation on a bounded sample."""
+def cpu_baseline(wl, seconds=10.0):
+    """Time the reference's CPU implementation on a bounded sample (~10 s of
+    CPU work: whole passes over the workload, or a prefix of it)."""
     import oracle as O
 
     impl, kind = ("ref", "reference") if O.ref_available() else ("orc", "port")
     n_total = wl.units()
-    count = min(n_total, 2048)
     t0 = time.perf_counter()
-    wl.cpu_run(impl, count)
-    dt = time.perf_counter() - t0
-    target = min(n_total, max(count, int(count * (max_seconds / 3) / max(dt, 1e-6))))
-    t0 = time.perf_counter()
-    wl.cpu_run(impl, target)
-    dt = time.perf_counter() - t0
+    got = wl.cpu_run(impl, min(n_total, wl.cpu_probe_units))
+    dt = max(time.perf_counter() - t0, 1e-6)
+    target = min(n_total, max(got, int(got * seconds / 2 / dt)))
+    passes, done, t0 = 0, 0, time.perf_counter()
+    while True:
+        done += wl.cpu_run(impl, target)
+        passes += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or passes >= 1000:
+            break
     src = ("reference headers include/mpc_cuda/cu_freal.cuh + cu_fcomplex.cuh built for the host "
            "(oracle/_ref), OpenMP" if kind == "reference" else "oracle C restatement, OpenMP")
-    return {"value": target / dt, "unit": "mp-FMA/s", "cores": O.num_threads(), "kind": kind,
-            "sample": f"{target} of {n_total} elements of the same workload, {dt:.2f} s; {src}"}
+    return {"value": done / el, "unit": "mp-FMA/s", "cores": O.num_threads(), "kind": kind,
+            "sample": f"{passes} pass(es) over {target} of {n_total} units of the same workload, "
+                      f"{el:.1f} s; {src}"}
 
 
 def run_reference(args):
@@ -282,25 +444,26 @@ def run_reference(args):
     import oracle as O
 
     impl, kind = ("ref", "reference") if O.ref_available() else ("orc", "port")
-    count = min(wl.units(), 2048)
     t0 = time.perf_counter()
-    wl.cpu_run(impl, count)
-    dt = time.perf_counter() - t0
-    per_step = min(wl.units(), max(count, int(count * 8.0 / max(args.steps + args.warmup, 1) / max(dt, 1e-6))))
+    got = wl.cpu_run(impl, min(wl.units(), wl.cpu_probe_units))
+    dt = max(time.perf_counter() - t0, 1e-6)
+    per_step = min(wl.units(), max(got, int(got * 30.0 / max(args.steps + args.warmup, 1) / dt)))
     for _ in range(args.warmup):
         wl.cpu_run(impl, per_step)
+    done = 0
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        wl.cpu_run(impl, per_step)
+        done += wl.cpu_run(impl, per_step)
     dt = time.perf_counter() - t0
-    value = per_step * args.steps / dt
+    per_step = done // args.steps
+    value = done / dt
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "mp-FMA/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic", "config": wl.config(),
         "cpu_baseline": {"value": value, "unit": "mp-FMA/s", "cores": O.num_threads(), "kind": kind,
-                         "sample": f"{per_step} of {wl.units()} elements per step"},
+                         "sample": f"{per_step} of {wl.units()} units per step"},
         "e2e": {"value": value, "unit": "mp-FMA/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -347,6 +510,10 @@ def run_gpu(args):
     torch.cuda.synchronize()
     if clocks:
         clocks.start()
+    M = wl.M
+    profiled = hasattr(wl, "roofline_tensor")
+    if profiled:
+        M.lib().mpb_profile_enable(1)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for i in range(args.steps):
@@ -356,6 +523,11 @@ def run_gpu(args):
     ms = e0.elapsed_time(e1)
     barrier()
     clk = clocks.stop() if clocks else None
+    tensor_ms = None
+    if profiled:
+        cnt = M.lib().mpb_profile_phase_count(2)
+        tensor_ms = M.lib().mpb_profile_phase_ms(2) / max(cnt, 1)
+        M.lib().mpb_profile_enable(0)
     ms_max = max_over_ranks(ms)
     kernel_s = ms / args.steps / 1e3
 
@@ -377,9 +549,12 @@ def run_gpu(args):
     units = wl.units() * world * args.steps
     if rank == 0:
         peaks = measured_peaks()
-        ipk = imad_peak(sp)
-        roof = wl.roofline(kernel_s, peaks, ipk)
-        cpu = cpu_baseline(wl) if world == 1 else None
+        extra = wl.extra(sp) if hasattr(wl, "extra") else None
+        if profiled:
+            roof = wl.roofline_tensor(tensor_ms, int8_peak_ops(device))
+        else:
+            roof = wl.roofline(kernel_s, peaks, imad_peak(sp))
+        cpu = cpu_baseline(wl) if world == 1 and not args.no_cpu else None
         h2d, d2h = wl.e2e_bytes()
         line = {
             "metric": METRIC, "value": units / (ms_max / 1e3), "unit": "mp-FMA/s", "n_gpus": world,
@@ -395,6 +570,12 @@ def run_gpu(args):
             "gpu_launches_e2e": wl.e2e_launches_per_step * args.steps,
             "clocks": clk,
         }
+        if extra:
+            line["plain"] = {"value": extra["plain_value"], "unit": "mp-FMA/s",
+                             "ms_per_step": extra["plain_ms_per_step"],
+                             "kernel": "k_gemm_r (sequential-k, per-operation rounding)"}
+            line["exact_over_plain"] = line["value"] / extra["plain_value"]
+            line["status"] = {"fallback_rows_cols": extra["status"][0], "kernel_error": extra["status"][1]}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -405,13 +586,17 @@ def run_gpu(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: the workload's, about 2 s of GPU time)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("mpb", "reference"), default="mpb")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.steps is None:
+        args.steps = WORKLOADS[args.workload]().default_steps
     if args.impl == "reference":
         return run_reference(args)
     return run_gpu(args)

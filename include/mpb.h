@@ -50,6 +50,19 @@ int mpb_version(void);                         /* major*10000 + minor*100 + patc
 const char *mpb_status_string(int status);
 int mpb_prec_supported(int prec);              /* 1 if prec is one of the supported values */
 
+/* ---- opt-in phase timing (profiling aid; off by default) ----
+ * mpb_profile_enable(1) clears previous records and makes multi-kernel entry
+ * points (mpb_gemm_exact_r) record a CUDA event pair around each phase on the
+ * caller's stream: 0 exponent statistics, 1 slicing, 2 tensor-core GEMM,
+ * 3 exact rounding, 4 fallback.  mpb_profile_phase_ms waits for the recorded
+ * events and returns the phase's total time in ms over every call since
+ * enabling (-1 if none); mpb_profile_phase_count returns the number of calls
+ * recorded.  Not thread-safe against concurrent enable.  No counterpart in the
+ * reference. */
+void mpb_profile_enable(int on);
+float mpb_profile_phase_ms(int phase);
+int mpb_profile_phase_count(int phase);
+
 /* ---- layout ---- */
 size_t mpb_vec_bytes(int prec, size_t n);      /* real vector, 0 for unsupported prec */
 size_t mpb_cvec_bytes(int prec, size_t n);     /* complex vector */
@@ -99,6 +112,22 @@ int mpb_gemm_r(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda
                void *C, size_t ldc, void *stream);
 int mpb_gemm_c(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
                void *C, size_t ldc, void *stream);
+
+/* ---- exact-accumulation GEMM on the INT8 tensor cores (no counterpart in the reference) ---- */
+/* C[i,j] = RNDN(sum_k A[i,k]*B[k,j]) with ONE rounding per entry: the correctly
+ * rounded dot product (MPFR mpfr_dot semantics; <= 0.5 ULP).  Each row of A and
+ * column of B is aligned to its largest exponent; entries more than sp_bits
+ * below it do not fit the slice budget, and such rows / columns are computed
+ * by the plain per-operation-rounded kernel instead (never on the CPU).
+ * workspace: device scratch of mpb_gemm_exact_workspace(...) bytes, 256-byte
+ * aligned, owned by the caller; calls sharing a workspace must not overlap.
+ * status: optional device int[2], written asynchronously: [0] = number of rows
+ * plus columns that took the fallback, [1] = 0 or an internal kernel error code.
+ * The slice budget costs S^2 int8 tensor-core products per multiply-add,
+ * S = ceil((prec + sp_bits + 2) / 8); sp_bits <= 118 is supported. */
+size_t mpb_gemm_exact_workspace(int prec, size_t m, size_t n, size_t k, int sp_bits);
+int mpb_gemm_exact_r(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
+                     void *C, size_t ldc, int sp_bits, void *workspace, size_t ws_bytes, int *status, void *stream);
 
 #ifdef __cplusplus
 }

@@ -64,6 +64,11 @@ _SIGS = {
     "mpb_gemv_c": ([_I, _S, _S, _V, _S, _V, _V, _V, _V], C.c_int),
     "mpb_gemm_r": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _V], C.c_int),
     "mpb_gemm_c": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _V], C.c_int),
+    "mpb_gemm_exact_workspace": ([_I, _S, _S, _S, _I], C.c_size_t),
+    "mpb_profile_enable": ([_I], None),
+    "mpb_profile_phase_ms": ([_I], C.c_float),
+    "mpb_profile_phase_count": ([_I], C.c_int),
+    "mpb_gemm_exact_r": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _I, _V, _S, _V, _V], C.c_int),
 }
 
 
@@ -202,8 +207,31 @@ def gemm(prec, m, n, k, A, lda, B, ldb, Cm, ldc, cplx=False, stream=None):
           _stream(stream))
 
 
+def gemm_exact_workspace(prec, m, n, k, sp_bits=32):
+    return int(lib().mpb_gemm_exact_workspace(prec, m, n, k, sp_bits))
+
+
+def gemm_exact(prec, m, n, k, A, lda, B, ldb, Cm, ldc, sp_bits=32, workspace=None, status=None,
+               cplx=False, stream=None):
+    """C = A.B with one rounding per entry (exact accumulation on the INT8
+    tensor cores).  ``workspace``: device buffer of gemm_exact_workspace(...)
+    bytes (allocated here when None); ``status``: optional device int32[2]
+    receiving [fallback rows+cols, kernel error code]."""
+    if cplx:
+        raise NotImplementedError("complex exact GEMM: use gemm_exact_c")
+    if workspace is None:
+        import torch
+
+        nbytes = gemm_exact_workspace(prec, m, n, k, sp_bits)
+        workspace = torch.empty(max(nbytes, 256), dtype=torch.uint8, device="cuda")
+    nbytes = workspace.numel() * workspace.element_size() if not isinstance(workspace, int) else (1 << 62)
+    _call("mpb_gemm_exact_r", prec, m, n, k, _ptr(A), lda, _ptr(B), ldb, _ptr(Cm), ldc, sp_bits, _ptr(workspace),
+          nbytes, _ptr(status), _stream(stream))
+    return workspace
+
+
 __all__ = [
     "SUPPORTED", "MpbError", "aos_bytes", "tile_bytes", "vec_bytes", "build", "lib", "host_lib", "empty",
     "empty_matrix", "pack_aos", "unpack_aos", "from_double", "to_double", "binop", "fma", "axpy", "gemv", "gemm",
-    "layout", "MPB_OP_MUL", "MPB_OP_ADD", "MPB_OP_SUB",
+    "layout", "MPB_OP_MUL", "MPB_OP_ADD", "MPB_OP_SUB", "gemm_exact", "gemm_exact_workspace",
 ]

@@ -1,5 +1,8 @@
 /* capi.cu -- library information and layout queries of the mpb C ABI. */
+#include <atomic>
 #include <mutex>
+#include <utility>
+#include <vector>
 
 #include "common.cuh"
 
@@ -18,7 +21,71 @@ int sm_count() {
   return cached[dev];
 }
 
+/* ---------------- opt-in phase timing ---------------- */
+/* Each recorded interval is an event pair taken from a growing pool; the
+ * intervals of every call since mpb_profile_enable(1) are kept and summed. */
+static std::atomic<int> g_profile{0};
+static std::mutex g_prof_mu;
+static std::vector<cudaEvent_t> g_pool;
+static size_t g_pool_used = 0;
+static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_iv[kPhases];
+static cudaEvent_t g_open[kPhases];
+
+static cudaEvent_t next_event() {
+  if (g_pool_used == g_pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    g_pool.push_back(e);
+  }
+  return g_pool[g_pool_used++];
+}
+
+void profile_mark(int phase, bool begin, cudaStream_t st) {
+  if (!g_profile.load(std::memory_order_relaxed) || phase < 0 || phase >= kPhases) return;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  cudaEvent_t e = next_event();
+  if (!e) return;
+  cudaEventRecord(e, st);
+  if (begin)
+    g_open[phase] = e;
+  else if (g_open[phase])
+    g_iv[phase].emplace_back(g_open[phase], e), g_open[phase] = nullptr;
+}
+
 } /* namespace mpb */
+
+extern "C" void mpb_profile_enable(int on) {
+  using namespace mpb;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (int p = 0; p < kPhases; ++p) {
+    g_iv[p].clear();
+    g_open[p] = nullptr;
+  }
+  g_pool_used = 0;
+  g_profile.store(on ? 1 : 0);
+}
+
+extern "C" float mpb_profile_phase_ms(int phase) {
+  using namespace mpb;
+  if (phase < 0 || phase >= kPhases) return -1.0f;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (g_iv[phase].empty()) return -1.0f;
+  double total = 0.0;
+  for (auto &iv : g_iv[phase]) {
+    float ms = 0.0f;
+    if (cudaEventSynchronize(iv.second) != cudaSuccess) return -1.0f;
+    if (cudaEventElapsedTime(&ms, iv.first, iv.second) != cudaSuccess) return -1.0f;
+    total += ms;
+  }
+  return (float)total;
+}
+
+extern "C" int mpb_profile_phase_count(int phase) {
+  using namespace mpb;
+  if (phase < 0 || phase >= kPhases) return 0;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  return (int)g_iv[phase].size();
+}
 
 extern "C" int mpb_version(void) { return 100; }
 

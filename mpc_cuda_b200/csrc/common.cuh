@@ -36,6 +36,11 @@ inline int launch_status() {
 /* SM count of the current device (cached per device) */
 int sm_count();
 
+/* Opt-in phase timing (mpb_profile_enable): entry points that run several
+ * kernels record a CUDA event pair around each phase on the caller's stream. */
+enum { kPhaseStats = 0, kPhaseSlice = 1, kPhaseTensor = 2, kPhaseRound = 3, kPhaseFallback = 4, kPhases = 5 };
+void profile_mark(int phase, bool begin, cudaStream_t st);
+
 /* Grid for a grid-stride kernel over `work` warp-sized units of 32 threads
  * each: enough blocks to fill every SM at the kernel's occupancy, never more
  * than the work needs. */

@@ -49,8 +49,15 @@ __global__ void __launch_bounds__(kBlock) k_pack_aos(size_t n, int cplx, const u
   const size_t es = 16u + 4u * N;
   const size_t np = tiles_for(n) * 32u;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
-    if (i >= n) continue;
     fval<N> re, im;
+    if (i >= n) { /* padding lanes of the last tile hold canonical zeros */
+      set_zero(re);
+      if (cplx)
+        store_celem<N>(vec, i, re, re);
+      else
+        store_elem<N>(vec, i, re);
+      continue;
+    }
     if (cplx) {
       aos_read<N>(re, aos + i * 2u * es);
       aos_read<N>(im, aos + i * 2u * es + es);
@@ -213,27 +220,38 @@ __global__ void __launch_bounds__(kBlock) k_axpy_r(size_t n, const uint8_t *a, c
 }
 /* complex z = a*x + y: re = round(xr*ar - xi*ai), im = round(xr*ai + xi*ar)
  * from exact products (the scalar as row multiplier again), then the
- * component-wise rounded add of y. */
+ * component-wise rounded add of y.  Both components share the x operands and
+ * differ only in which part of a multiplies them, so the body runs as a
+ * two-trip loop over the component with the a parts picked by pointer: one
+ * copy of the product/rounding code instead of two keeps the loop inside the
+ * instruction cache at high precision. */
 template <int N>
 __global__ void __launch_bounds__(kBlock) k_axpy_c(size_t n, const uint8_t *a, const uint8_t *x, const uint8_t *y,
                                                    uint8_t *z) {
-  __shared__ fval<N> sar, sai;
+  __shared__ fval<N> sa[2];
   if (threadIdx.x == 0) {
     fval<N> tr, ti;
     load_celem<N>(tr, ti, a, 0);
-    sar = tr;
-    sai = ti;
+    sa[0] = tr;
+    sa[1] = ti;
   }
   __syncthreads();
   const size_t np = tiles_for(n) * 32u;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
-    fval<N> xr, xi, tr, ti, yr, yi, rr, ri;
+    fval<N> xr, xi;
     load_celem<N, kStream>(xr, xi, x, i);
-    cmul<N, true>(tr, ti, xr, xi, sar, sai);
-    load_celem<N, kStream>(yr, yi, y, i);
-    add<N, true>(rr, tr, yr);
-    add<N, true>(ri, ti, yi);
-    if (i < n) store_celem<N, kStream>(z, i, rr, ri);
+    const size_t ct = (i >> 5) * 2u * sol<N>::kTileBytes;
+#pragma unroll 1
+    for (int comp = 0; comp < 2; ++comp) {
+      /* re: xr*ar - xi*ai ; im: xr*ai + xi*ar */
+      const fval<N> &a1 = sa[comp];
+      const fval<N> &a2 = sa[comp ^ 1];
+      fval<N> t, yv, r;
+      fmms<N, true>(t, xr, a1, xi, a2, comp == 0 ? 1u : 0u);
+      load_elem<N, kStream>(yv, y + ct + comp * sol<N>::kTileBytes, i & 31u);
+      add<N, true>(r, t, yv);
+      if (i < n) store_elem<N, kStream>(z + ct + comp * sol<N>::kTileBytes, i & 31u, r);
+    }
   }
 }
 

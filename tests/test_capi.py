@@ -67,3 +67,19 @@ def test_empty_inputs_are_noops(mpb):
     assert L.mpb_gemm_r(512, 0, 8, 8, None, 32, None, 32, None, 32, None) == 0
     assert L.mpb_gemv_c(256, 0, 5, None, 32, None, None, None, None) == 0
     assert L.mpb_pack_aos(256, 0, None, None, None) == 0
+
+
+def test_exact_gemm_workspace_and_checks(mpb):
+    L = mpb.lib()
+    # PB=512, 1024^3, 32-bit spread: S = 69 digit planes, 137 diagonals
+    S, m = 69, 1024
+    need = L.mpb_gemm_exact_workspace(512, m, m, m, 32)
+    planes = S * 2 * m * m + 137 * m * m * 4
+    assert planes <= need <= planes + 64 * 1024
+    assert L.mpb_gemm_exact_workspace(96, 8, 8, 8, 32) == 0
+    good = 4096
+    # missing workspace, misaligned workspace, bad leading dimension
+    assert L.mpb_gemm_exact_r(512, 8, 8, 8, good, 32, good, 32, good, 32, 32, None, 0, None, None) == -8
+    assert L.mpb_gemm_exact_r(512, 8, 8, 8, good, 32, good, 32, good, 32, 32, good + 16, 1 << 30, None, None) == -4
+    assert L.mpb_gemm_exact_r(512, 8, 8, 8, good, 40, good, 32, good, 32, 32, good, 1 << 30, None, None) == -5
+    assert L.mpb_gemm_exact_r(512, 0, 8, 8, None, 32, None, 32, None, 32, 32, None, 0, None, None) == 0

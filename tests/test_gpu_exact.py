@@ -1,0 +1,121 @@
+"""Exact-accumulation GEMM on the INT8 tensor cores, through the C ABI.
+
+Every entry is one rounding of the exact dot product, so it must equal the
+system MPFR's mpfr_dot (the correctly rounded dot, pinned in test_oracle.py)
+bit for bit, and lie within 0.5 ULP of a 4*PB oracle.  Rows/columns outside
+the spread budget are computed by the plain per-operation kernel and must
+equal the sequential-k MPFR oracle instead.
+"""
+import numpy as np
+import pytest
+
+from conftest import to_dev, to_host
+from mpc_cuda_b200 import layout, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def rand_aos(prec, count, seed, elo=-8, ehi=8, zero_frac=0.05):
+    rng = np.random.default_rng(seed)
+    return layout.aos_from_parts(prec, *synth.random_elems(rng, prec, count, elo, ehi, zero_frac))
+
+
+def pad_rows(prec, A, rows, cols, ld):
+    es = A.shape[1]
+    z = layout.aos_from_parts(prec, np.zeros((1, prec // 32), np.uint32), np.array([layout.HEAD_ZERO], np.uint32))
+    out = np.repeat(z, rows * ld, axis=0).reshape(rows, ld, es)
+    out[:, :cols] = A.reshape(rows, cols, es)
+    return out.reshape(rows * ld, es)
+
+
+def run_exact(mpb, prec, m, n, k, A, B, sp_bits):
+    import torch
+
+    lda, ldb, ldc = (-(-k // 32) * 32, -(-n // 32) * 32, -(-n // 32) * 32)
+    dA = to_dev(layout.aos_to_vec(prec, pad_rows(prec, A, m, k, lda)))
+    dB = to_dev(layout.aos_to_vec(prec, pad_rows(prec, B, k, n, ldb)))
+    Cd = mpb.empty(prec, m * ldc)
+    st = torch.zeros(2, dtype=torch.int32, device="cuda")
+    mpb.gemm_exact(prec, m, n, k, dA, lda, dB, ldb, Cd, ldc, sp_bits=sp_bits, status=st)
+    C = layout.vec_to_aos(prec, to_host(Cd), m * ldc).reshape(m, ldc, -1)[:, :n].reshape(m * n, -1)
+    return C, st.cpu().numpy()
+
+
+@pytest.mark.parametrize("prec", (64, 256, 512, 1024, 2048))
+@pytest.mark.parametrize("shape", ((1, 1, 1), (5, 7, 33), (33, 40, 17), (128, 256, 128), (130, 260, 300)))
+def test_exact_vs_mpfr_dot(orc, mpb, prec, shape):
+    m, n, k = shape
+    if prec == 2048 and m * n * k > 200000:
+        pytest.skip("covered at smaller shapes")
+    A = rand_aos(prec, m * k, 100 + m + prec)
+    B = rand_aos(prec, k * n, 200 + n + prec)
+    C, st = run_exact(mpb, prec, m, n, k, A, B, sp_bits=16)
+    assert st[1] == 0, f"kernel error code {st[1]}"
+    assert st[0] == 0, "no row/column exceeds a 16-bit spread here"
+    exp = orc.gemm_exact(prec, m, n, k, A, k, B, n, impl="mp")
+    bad, first = orc.mismatches(prec, C, exp)
+    assert bad == 0, f"PB={prec} {shape}: {bad} mismatches, first at {first}"
+
+
+@pytest.mark.parametrize("prec", (128, 512))
+def test_exact_cancellation_and_signs(orc, mpb, prec):
+    """Columns of B that are exact negatives of each other give exact zeros and
+    deep cancellation; the result must still be the correctly rounded sum."""
+    m, n, k = 40, 64, 96
+    A = rand_aos(prec, m * k, 7, -4, 4, 0.0)
+    B = rand_aos(prec, k * n, 8, -4, 4, 0.0).reshape(k, n, -1)
+    B[:, 1] = B[:, 0]
+    B[:, 1, 0:4] = np.where(B[:, 0, 0:4].view(np.int32) > 0, -1, 1).astype(np.int32).view(np.uint8).reshape(k, 4)
+    B[:, 3] = B[:, 2]
+    B = B.reshape(k * n, -1)
+    C, st = run_exact(mpb, prec, m, n, k, A, B, sp_bits=8)
+    assert st[1] == 0
+    exp = orc.gemm_exact(prec, m, n, k, A, k, B, n, impl="mp")
+    assert orc.mismatches(prec, C, exp)[0] == 0
+
+
+def test_exact_fallback_rows_and_columns(orc, mpb):
+    """Rows/columns whose exponent spread exceeds the budget take the plain
+    per-operation-rounded kernel (never the CPU) and are counted."""
+    prec, m, n, k = 256, 20, 40, 50
+    A = rand_aos(prec, m * k, 31, -4, 4, 0.0).reshape(m, k, -1)
+    B = rand_aos(prec, k * n, 32, -4, 4, 0.0).reshape(k, n, -1)
+    for r in (3, 11):  # one tiny entry far below the row's top
+        A[r, 5, 8:16] = np.array([-400], np.int64).view(np.uint8)
+    B[7, 9, 8:16] = np.array([-400], np.int64).view(np.uint8)
+    A, B = A.reshape(m * k, -1), B.reshape(k * n, -1)
+    C, st = run_exact(mpb, prec, m, n, k, A, B, sp_bits=32)
+    assert st[1] == 0 and st[0] == 3
+    exact = orc.gemm_exact(prec, m, n, k, A, k, B, n, impl="mp").reshape(m, n, -1)
+    plain = orc.gemm(prec, m, n, k, A, k, B, n, impl="mp").reshape(m, n, -1)
+    C = C.reshape(m, n, -1)
+    for i in range(m):
+        for j in range(n):
+            want = plain if (i in (3, 11) or j == 9) else exact
+            assert orc.mismatches(prec, C[i, j:j + 1], want[i, j:j + 1])[0] == 0, (i, j)
+
+
+def test_exact_real_pb512_full_size(orc, mpb):
+    """The 1024^3 PB=512 workload: entries with 16 random limbs and exponents
+    in [-16, 16]; a row sample must equal mpfr_dot and be <= 0.5 ULP from the
+    exact sum at 2048 bits."""
+    import torch
+
+    prec, m, n, k = 512, 1024, 1024, 1024
+    (al, ah), (bl, bh) = synth.gemm_r512()
+    dA = to_dev(layout.vec_from_parts(prec, al, ah))
+    dB = to_dev(layout.vec_from_parts(prec, bl, bh))
+    Cd = mpb.empty(prec, m * n)
+    st = torch.zeros(2, dtype=torch.int32, device="cuda")
+    mpb.gemm_exact(prec, m, n, k, dA, k, dB, n, Cd, n, sp_bits=32, status=st)
+    st = st.cpu().numpy()
+    assert st[1] == 0 and st[0] == 0
+    got = layout.vec_to_aos(prec, to_host(Cd), m * n)
+    A, B = layout.aos_from_parts(prec, al, ah), layout.aos_from_parts(prec, bl, bh)
+    for r0, r1 in ((0, 2), (517, 518), (m - 1, m)):
+        exp = orc.gemm_exact(prec, m, n, k, A, k, B, n, impl="mp", rows=(r0, r1))
+        sel = slice(r0 * n, r1 * n)
+        assert orc.mismatches(prec, got[sel], exp[sel])[0] == 0
+        e4 = orc.gemm_exact(prec, m, n, k, A, k, B, n, out_prec=4 * prec, rows=(r0, r1))
+        ulp = orc.ulp_errors(prec, got[sel], 4 * prec, e4[r0 * n * 1:r1 * n])
+        assert ulp.max() <= 0.5
