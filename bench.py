@@ -2,7 +2,7 @@
 """bench.py -- throughput of the mpb engine on its benchmark workloads.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpb|reference]
-                    [--workload axpy_c1024|axpy_r256|...]
+                    [--workload gemm_r512|axpy_c1024|axpy_r256]
 
 One JSON line on stdout (rank 0).  A step is one pass of the hot path over
 one batch of synthetic operands already resident in HBM; K steps are timed
@@ -292,7 +292,7 @@ class GemmWorkload:
 
     @property
     def default_steps(self):
-        return 20
+        return 200  # ~1 s of GPU time: long enough for clock sampling
 
     launches_per_step = 7  # stats x2, slice x2, tensor-core GEMM, round, fallback
     e2e_launches_per_step = 10
@@ -406,7 +406,7 @@ WORKLOADS = {
     "gemm_r512": lambda: GemmWorkload("gemm_r512", 512, 1024, 1024, 1024, 32,
                                       lambda seed: __import__("mpc_cuda_b200.synth", fromlist=["x"]).gemm_r512(seed)),
 }
-DEFAULT_WORKLOAD = "axpy_c1024"
+DEFAULT_WORKLOAD = "gemm_r512"
 
 
 # ------------------------------------------------------------------ CPU side
