@@ -128,6 +128,17 @@ int mpb_gemm_c(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda
 size_t mpb_gemm_exact_workspace(int prec, size_t m, size_t n, size_t k, int sp_bits);
 int mpb_gemm_exact_r(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
                      void *C, size_t ldc, int sp_bits, void *workspace, size_t ws_bytes, int *status, void *stream);
+/* The same exact GEMM for callers that cannot allocate device memory (a
+ * latency-critical loop that must not call cudaMalloc after start-up, or a
+ * framework that owns the whole memory pool): no workspace argument and no
+ * allocation; the scratch is a fixed 16 MiB area inside the library, reserved
+ * on every GPU that loads it.  Problems needing more scratch than that
+ * (mpb_gemm_exact_workspace(...) > 16 MiB) return MPB_ERR_SIZE.  The first call
+ * on a device looks the area up and should come before any stream capture.
+ * All calls share the area, so calls that overlap on the GPU race.  No
+ * counterpart in the reference. */
+int mpb_gemm_exact_r_static(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B,
+                            size_t ldb, void *C, size_t ldc, int sp_bits, int *status, void *stream);
 
 #ifdef __cplusplus
 }

@@ -69,6 +69,7 @@ _SIGS = {
     "mpb_profile_phase_ms": ([_I], C.c_float),
     "mpb_profile_phase_count": ([_I], C.c_int),
     "mpb_gemm_exact_r": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _I, _V, _S, _V, _V], C.c_int),
+    "mpb_gemm_exact_r_static": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _I, _V, _V], C.c_int),
 }
 
 

@@ -773,3 +773,69 @@ extern "C" int mpb_gemm_exact_r(int prec, size_t m, size_t n, size_t k, const vo
   });
   return MPB_OK;
 }
+
+/* ------------------------------------------------------------------ *
+ * Exact GEMM without any allocation.
+ *
+ * For callers that cannot call cudaMalloc: code that runs after start-up in
+ * a latency-critical loop where an allocation (and its implicit device
+ * synchronisation) is not allowed, or code inside a framework that owns the
+ * whole device memory pool so a foreign cudaMalloc would fail or fragment it.
+ * Such callers still pass A, B and C; the scratch the exact GEMM needs (digit
+ * planes, diagonal planes, statistics) comes from this fixed area instead of
+ * a caller-provided workspace.
+ *
+ * kStaticScratchBytes (16 MiB) is reserved on every GPU that loads this
+ * library, for the life of the process.  Problems whose
+ * mpb_gemm_exact_workspace(...) exceeds it are rejected with MPB_ERR_SIZE
+ * (e.g. PB=512 up to about 128 x 128 x 128).  Every call shares the area: calls
+ * that overlap on the GPU (other streams, other host threads) race and must
+ * be serialised by the caller.  The counters that must start at zero are
+ * cleared by each call; everything else is overwritten.
+ * ------------------------------------------------------------------ */
+namespace {
+constexpr size_t kStaticScratchBytes = (size_t)16 << 20;
+static __device__ __align__(256) uint8_t g_exact_scratch[kStaticScratchBytes];
+
+/* Device address of g_exact_scratch on the current device.  The host-side
+ * name is only a stand-in, so the address is looked up once per device (the
+ * first call on a device, which should therefore come before any stream
+ * capture) with that device current. */
+uint8_t *static_scratch() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  static std::once_flag once[64];
+  static uint8_t *addr[64];
+  std::call_once(once[dev], [dev] {
+    void *p = nullptr;
+    addr[dev] = (cudaGetSymbolAddress(&p, g_exact_scratch) == cudaSuccess) ? (uint8_t *)p : nullptr;
+  });
+  return addr[dev];
+}
+}  // namespace
+
+extern "C" int mpb_gemm_exact_r_static(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda,
+                                       const void *B, size_t ldb, void *C, size_t ldc, int sp_bits, int *status,
+                                       void *stream) {
+  if (!prec_ok(prec)) return MPB_ERR_PREC;
+  if (m == 0 || n == 0) return MPB_OK;
+  if (m > (1u << 24) || n > (1u << 24) || k > (1u << 24)) return MPB_ERR_SIZE;
+  if (ldc % 32 || ldc < n) return MPB_ERR_LD;
+  if (k > 0 && (lda % 32 || lda < k || ldb % 32 || ldb < n)) return MPB_ERR_LD;
+  if (!C || (k > 0 && (!A || !B))) return MPB_ERR_NULL;
+  if (!aligned16(C) || (k > 0 && (!aligned16(A) || !aligned16(B)))) return MPB_ERR_ALIGN;
+  if (k == 0) return mpb_gemm_r(prec, m, n, 0, nullptr, 32, nullptr, 32, C, ldc, stream);
+  exact::Plan p;
+  if (!exact::make_plan(prec, m, n, k, sp_bits, p) || p.XL > 4) return MPB_ERR_ARG;
+  if (p.total > kStaticScratchBytes) return MPB_ERR_SIZE; /* larger than the static scratch area */
+  uint8_t *ws = static_scratch();
+  if (!ws) return MPB_ERR_CUDA;
+  cudaStream_t st = as_stream(stream);
+  MPB_DISPATCH_PREC(prec, {
+    MPB_EXACT_XL(p.XL, {
+      return exact::run_exact<N, XLC>(p, (const uint8_t *)A, lda, (const uint8_t *)B, ldb, (uint8_t *)C, ldc, ws,
+                                      status, st);
+    });
+  });
+  return MPB_OK;
+}
