@@ -2,7 +2,7 @@
 """bench.py -- throughput of the mpb engine on its benchmark workloads.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpb|reference]
-                    [--workload gemm_r512|axpy_c1024|axpy_r256]
+                    [--workload gemm_r512|gemm_c256|axpy_c1024|axpy_r256]
 
 One JSON line on stdout (rank 0).  A step is one pass of the hot path over
 one batch of synthetic operands already resident in HBM; K steps are timed
@@ -283,12 +283,15 @@ class GemmWorkload:
     tensor-core GEMM (one rounding per entry) is the timed step; the plain
     per-operation-rounded kernel on the same operands is timed beside it."""
 
-    def __init__(self, name, prec, m, n, k, sp_bits, gen):
+    def __init__(self, name, prec, m, n, k, sp_bits, gen, cplx=False):
         self.name, self.prec, self.m, self.n, self.k, self.sp_bits, self.gen = name, prec, m, n, k, sp_bits, gen
-        self.cplx = False
-        self.S = (prec + sp_bits + 2 + 7) // 8
-        self.desc = (f"real matmul C=A.B, cu_freal<{prec}>, {m}x{n}x{k}: exact-accumulation GEMM on INT8 "
-                     f"tensor cores (one rounding per entry, {self.S} digit slices) vs plain sequential-k kernel")
+        self.cplx = cplx
+        self.nprod = 3 if cplx else 1  # complex: 3 exact real products (Gauss form)
+        self.S = (prec + sp_bits + (3 if cplx else 2) + 7) // 8
+        kind = f"complex matmul, cu_fcomplex<{prec}>" if cplx else f"real matmul, cu_freal<{prec}>"
+        form = ", 3-product Gauss form, one rounding per component" if cplx else ", one rounding per entry"
+        self.desc = (f"{kind} C=A.B, {m}x{n}x{k}: exact-accumulation GEMM on INT8 tensor cores "
+                     f"({self.S} digit slices{form}) vs plain sequential-k kernel")
 
     @property
     def default_steps(self):
@@ -300,9 +303,12 @@ class GemmWorkload:
     def make_host(self, rank):
         from mpc_cuda_b200 import layout
 
-        (al, ah), (bl, bh) = self.gen(seed=0x5EED3 + 1000 * rank)
-        self.parts = ((al, ah), (bl, bh))
-        return layout.aos_from_parts(self.prec, al, ah), layout.aos_from_parts(self.prec, bl, bh)
+        from mpc_cuda_b200 import synth
+
+        a, b = self.gen(seed=(0x5EED5 if self.cplx else 0x5EED3) + 1000 * rank)
+        if self.cplx:
+            return synth.interleave_complex(self.prec, *a), synth.interleave_complex(self.prec, *b)
+        return layout.aos_from_parts(self.prec, *a), layout.aos_from_parts(self.prec, *b)
 
     def setup(self, rank, device):
         import torch
@@ -313,12 +319,12 @@ class GemmWorkload:
         self.M = M
         A, B = self.make_host(rank)
         self.host = (A, B)
-        (al, ah), (bl, bh) = self.parts
-        self.dA = dev_from(layout.vec_from_parts(self.prec, al, ah), device)
-        self.dB = dev_from(layout.vec_from_parts(self.prec, bl, bh), device)
-        self.dC = M.empty(self.prec, self.m * self.n, device=device)
-        self.dC2 = M.empty(self.prec, self.m * self.n, device=device)
-        self.ws = torch.empty(M.gemm_exact_workspace(self.prec, self.m, self.n, self.k, self.sp_bits),
+        c = self.cplx
+        self.dA = dev_from(layout.aos_to_vec(self.prec, A, c), device)
+        self.dB = dev_from(layout.aos_to_vec(self.prec, B, c), device)
+        self.dC = M.empty(self.prec, self.m * self.n, c, device=device)
+        self.dC2 = M.empty(self.prec, self.m * self.n, c, device=device)
+        self.ws = torch.empty(M.gemm_exact_workspace(self.prec, self.m, self.n, self.k, self.sp_bits, c),
                               dtype=torch.uint8, device=device)
         self.status = torch.zeros(2, dtype=torch.int32, device=device)
         self.hA, self.hB = pinned_from(A), pinned_from(B)
@@ -326,25 +332,27 @@ class GemmWorkload:
         self.dA_aos = torch.empty(A.size, dtype=torch.uint8, device=device)
         self.dB_aos = torch.empty(B.size, dtype=torch.uint8, device=device)
         self.dC_aos = torch.empty(self.hC.numel(), dtype=torch.uint8, device=device)
-        self.eA = M.empty(self.prec, self.m * self.k, device=device)
-        self.eB = M.empty(self.prec, self.k * self.n, device=device)
+        self.eA = M.empty(self.prec, self.m * self.k, c, device=device)
+        self.eB = M.empty(self.prec, self.k * self.n, c, device=device)
 
     def units(self):
         return self.m * self.n * self.k
 
     def step(self, i, stream):
         self.M.gemm_exact(self.prec, self.m, self.n, self.k, self.dA, self.k, self.dB, self.n, self.dC, self.n,
-                          sp_bits=self.sp_bits, workspace=self.ws, status=self.status, stream=stream)
+                          sp_bits=self.sp_bits, workspace=self.ws, status=self.status, cplx=self.cplx,
+                          stream=stream)
 
     def e2e_step(self, i, stream):
         M = self.M
         self.dA_aos.copy_(self.hA, non_blocking=True)
         self.dB_aos.copy_(self.hB, non_blocking=True)
-        M.pack_aos(self.prec, self.m * self.k, self.dA_aos, self.eA, stream=stream)
-        M.pack_aos(self.prec, self.k * self.n, self.dB_aos, self.eB, stream=stream)
+        c = self.cplx
+        M.pack_aos(self.prec, self.m * self.k, self.dA_aos, self.eA, c, stream=stream)
+        M.pack_aos(self.prec, self.k * self.n, self.dB_aos, self.eB, c, stream=stream)
         M.gemm_exact(self.prec, self.m, self.n, self.k, self.eA, self.k, self.eB, self.n, self.dC, self.n,
-                     sp_bits=self.sp_bits, workspace=self.ws, status=self.status, stream=stream)
-        M.unpack_aos(self.prec, self.m * self.n, self.dC, self.dC_aos, stream=stream)
+                     sp_bits=self.sp_bits, workspace=self.ws, status=self.status, cplx=c, stream=stream)
+        M.unpack_aos(self.prec, self.m * self.n, self.dC, self.dC_aos, c, stream=stream)
         self.hC.copy_(self.dC_aos, non_blocking=True)
 
     def e2e_bytes(self):
@@ -355,12 +363,13 @@ class GemmWorkload:
         import torch
 
         M = self.M
-        M.gemm(self.prec, self.m, self.n, self.k, self.dA, self.k, self.dB, self.n, self.dC2, self.n, stream=stream)
+        c = self.cplx
+        M.gemm(self.prec, self.m, self.n, self.k, self.dA, self.k, self.dB, self.n, self.dC2, self.n, c, stream=stream)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(steps):
-            M.gemm(self.prec, self.m, self.n, self.k, self.dA, self.k, self.dB, self.n, self.dC2, self.n,
+            M.gemm(self.prec, self.m, self.n, self.k, self.dA, self.k, self.dB, self.n, self.dC2, self.n, c,
                    stream=stream)
         e1.record()
         torch.cuda.synchronize()
@@ -369,12 +378,12 @@ class GemmWorkload:
         return {"plain_ms_per_step": plain_ms, "plain_value": self.units() / (plain_ms / 1e3), "status": st}
 
     def roofline_tensor(self, tensor_ms, int8_ops):
-        ops = 2.0 * self.units() * self.S * self.S
+        ops = 2.0 * self.nprod * self.units() * self.S * self.S
         achieved = ops / (tensor_ms / 1e3)
         return {"bound": "tensor", "achieved": round(achieved / 1e12, 1), "unit": "TOP/s (int8)",
                 "peak": round(int8_ops / 1e12, 1) if int8_ops else None,
                 "frac": round(achieved / int8_ops, 4) if int8_ops else None,
-                "ops_per_unit": 2 * self.S * self.S, "kernel": "k_diag_gemm (tcgen05.mma kind::i8)",
+                "ops_per_unit": 2 * self.nprod * self.S * self.S, "kernel": "k_diag_gemm (tcgen05.mma kind::i8)",
                 "kernel_ms": round(tensor_ms, 4),
                 "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm), measured in this run",
                 "traffic": None}
@@ -386,7 +395,7 @@ class GemmWorkload:
 
         A, B = self.host
         rows = max(1, min(self.m, count // (self.n * self.k)))
-        O.gemm(self.prec, self.m, self.n, self.k, A, self.k, B, self.n, impl=impl, rows=(0, rows))
+        O.gemm(self.prec, self.m, self.n, self.k, A, self.k, B, self.n, self.cplx, impl=impl, rows=(0, rows))
         return rows * self.n * self.k
 
     @property
@@ -396,8 +405,9 @@ class GemmWorkload:
     def config(self):
         return {"workload": self.desc, "prec": self.prec, "m": self.m, "n": self.n, "k": self.k,
                 "sp_bits": self.sp_bits, "slices": self.S,
-                "units": "mp-FMA (one exact product accumulated)",
-                "l2": "operands 143 MB > L2; digit planes 145 MB and diagonal planes 575 MB stream through HBM"}
+                "units": ("complex mp-FMA (one complex product accumulated)" if self.cplx
+                          else "mp-FMA (one exact product accumulated)"),
+                "l2": "operands > L2 (143 MB real / 71 MB complex); digit and diagonal planes stream through HBM"}
 
 
 WORKLOADS = {
@@ -405,6 +415,9 @@ WORKLOADS = {
     "axpy_r256": lambda: AxpyWorkload("axpy_r256", False, 256, 1 << 20, 0x5EED1),
     "gemm_r512": lambda: GemmWorkload("gemm_r512", 512, 1024, 1024, 1024, 32,
                                       lambda seed: __import__("mpc_cuda_b200.synth", fromlist=["x"]).gemm_r512(seed)),
+    "gemm_c256": lambda: GemmWorkload("gemm_c256", 256, 512, 512, 512, 16,
+                                      lambda seed: __import__("mpc_cuda_b200.synth", fromlist=["x"]).gemm_c256(seed),
+                                      cplx=True),
 }
 DEFAULT_WORKLOAD = "gemm_r512"
 

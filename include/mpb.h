@@ -126,7 +126,15 @@ int mpb_gemm_c(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda
  * The slice budget costs S^2 int8 tensor-core products per multiply-add,
  * S = ceil((prec + sp_bits + 2) / 8); sp_bits <= 118 is supported. */
 size_t mpb_gemm_exact_workspace(int prec, size_t m, size_t n, size_t k, int sp_bits);
+size_t mpb_gemm_exact_c_workspace(int prec, size_t m, size_t n, size_t k, int sp_bits);
 int mpb_gemm_exact_r(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
+                     void *C, size_t ldc, int sp_bits, void *workspace, size_t ws_bytes, int *status, void *stream);
+/* complex: each component rounded once (MPC mpc_dot semantics), computed in
+ * the 3-multiplication form re = T0 - T1, im = T2 - T0 - T1 on exact integers
+ * (T0 = Ar.Br, T1 = Ai.Bi, T2 = (Ar+Ai).(Br+Bi)); S = ceil((prec+sp_bits+3)/8).
+ * Complex operands and result use complex tiles; workspace size from
+ * mpb_gemm_exact_c_workspace. */
+int mpb_gemm_exact_c(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
                      void *C, size_t ldc, int sp_bits, void *workspace, size_t ws_bytes, int *status, void *stream);
 /* The same exact GEMM for callers that cannot allocate device memory (a
  * latency-critical loop that must not call cudaMalloc after start-up, or a

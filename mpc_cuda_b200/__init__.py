@@ -69,6 +69,8 @@ _SIGS = {
     "mpb_profile_phase_ms": ([_I], C.c_float),
     "mpb_profile_phase_count": ([_I], C.c_int),
     "mpb_gemm_exact_r": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _I, _V, _S, _V, _V], C.c_int),
+    "mpb_gemm_exact_c_workspace": ([_I, _S, _S, _S, _I], C.c_size_t),
+    "mpb_gemm_exact_c": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _I, _V, _S, _V, _V], C.c_int),
     "mpb_gemm_exact_r_static": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _I, _V, _V], C.c_int),
 }
 
@@ -208,8 +210,9 @@ def gemm(prec, m, n, k, A, lda, B, ldb, Cm, ldc, cplx=False, stream=None):
           _stream(stream))
 
 
-def gemm_exact_workspace(prec, m, n, k, sp_bits=32):
-    return int(lib().mpb_gemm_exact_workspace(prec, m, n, k, sp_bits))
+def gemm_exact_workspace(prec, m, n, k, sp_bits=32, cplx=False):
+    f = lib().mpb_gemm_exact_c_workspace if cplx else lib().mpb_gemm_exact_workspace
+    return int(f(prec, m, n, k, sp_bits))
 
 
 def gemm_exact(prec, m, n, k, A, lda, B, ldb, Cm, ldc, sp_bits=32, workspace=None, status=None,
@@ -218,16 +221,14 @@ def gemm_exact(prec, m, n, k, A, lda, B, ldb, Cm, ldc, sp_bits=32, workspace=Non
     tensor cores).  ``workspace``: device buffer of gemm_exact_workspace(...)
     bytes (allocated here when None); ``status``: optional device int32[2]
     receiving [fallback rows+cols, kernel error code]."""
-    if cplx:
-        raise NotImplementedError("complex exact GEMM: use gemm_exact_c")
     if workspace is None:
         import torch
 
-        nbytes = gemm_exact_workspace(prec, m, n, k, sp_bits)
+        nbytes = gemm_exact_workspace(prec, m, n, k, sp_bits, cplx)
         workspace = torch.empty(max(nbytes, 256), dtype=torch.uint8, device="cuda")
     nbytes = workspace.numel() * workspace.element_size() if not isinstance(workspace, int) else (1 << 62)
-    _call("mpb_gemm_exact_r", prec, m, n, k, _ptr(A), lda, _ptr(B), ldb, _ptr(Cm), ldc, sp_bits, _ptr(workspace),
-          nbytes, _ptr(status), _stream(stream))
+    _call("mpb_gemm_exact_c" if cplx else "mpb_gemm_exact_r", prec, m, n, k, _ptr(A), lda, _ptr(B), ldb, _ptr(Cm),
+          ldc, sp_bits, _ptr(workspace), nbytes, _ptr(status), _stream(stream))
     return workspace
 
 

@@ -1,0 +1,644 @@
+/* exact_gemm.cuh -- internal: plan, slicing and rounding kernels of the
+ * exact-accumulation GEMM, shared by the per-precision translation units
+ * exact_gemm_pb*.cu.  The algorithm is described in exact_gemm.cu. */
+#ifndef MPB_EXACT_GEMM_CUH
+#define MPB_EXACT_GEMM_CUH
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "common.cuh"
+#include "sm100.cuh"
+
+namespace mpb {
+namespace exact {
+
+constexpr int BM = 128;             /* output rows per tile (UMMA M) */
+constexpr int BN = 256;             /* output columns per tile (UMMA N) */
+constexpr int BK = 128;             /* K bytes per pipeline stage (one 128B swizzle row) */
+constexpr int STAGES = 4;
+constexpr uint32_t A_STAGE = BM * BK; /* 16 KB */
+constexpr uint32_t B_STAGE = BN * BK; /* 32 KB */
+constexpr int kGemmThreads = 192;   /* warp 0 TMA, warp 1 MMA, warps 2-5 epilogue */
+constexpr long kSafeTerms = 1L << 17; /* pairs * k < 2^17 keeps |D| < 2^31 */
+constexpr int kMaxParts = 16;       /* keeps the rounding's int64 word sums exact */
+constexpr size_t kSmemBytes = 1024 /* alignment slack */ + STAGES * (A_STAGE + B_STAGE) + 256 /* barriers */;
+
+/* the per-call geometry (host and device) */
+struct Plan {
+  int prec, N, S, SP, XL, cplx, nprod;
+  int m, n, k, kp, KC; /* kp = k padded to BK, KC = kp / BK chunks */
+  int P, cpp;          /* k-parts per diagonal, chunks per part */
+  int mt, nt;          /* tiles */
+  long units;
+  size_t off_rowE, off_colE, off_flags, off_cnt, off_asl, off_bsl, off_d, total;
+};
+
+static inline size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static bool make_plan(int prec, size_t m, size_t n, size_t k, int sp_bits, int cplx, Plan &p) {
+  if (sp_bits < 0 || sp_bits > 1024) return false;
+  const int guard = cplx ? 3 : 2;
+  p.prec = prec;
+  p.N = prec / 32;
+  p.cplx = cplx ? 1 : 0;
+  p.nprod = cplx ? 3 : 1;
+  p.S = (prec + sp_bits + guard + 7) / 8;
+  p.SP = 8 * p.S - prec - guard;
+  const int extra_bits = 8 * p.S - prec;
+  const int xl = (extra_bits + 31) / 32;
+  p.XL = xl <= 1 ? 1 : xl <= 2 ? 2 : xl <= 4 ? 4 : -1;
+  if (p.XL < 0) return false;
+  p.m = (int)m;
+  p.n = (int)n;
+  p.k = (int)k;
+  p.kp = (int)((k + BK - 1) / BK * BK);
+  p.KC = p.kp / BK;
+  const long terms = (long)p.S * p.kp;
+  p.P = (int)((terms + kSafeTerms - 1) / kSafeTerms);
+  if (p.P < 1) p.P = 1;
+  p.cpp = (p.KC + p.P - 1) / p.P;
+  p.P = (p.KC + p.cpp - 1) / p.cpp;
+  if (p.P > kMaxParts) return false;
+  p.mt = (int)((m + BM - 1) / BM);
+  p.nt = (int)((n + BN - 1) / BN);
+  p.units = (long)p.nprod * (2 * p.S - 1) * p.mt * p.nt * p.P;
+  size_t o = 0;
+  p.off_rowE = o;
+  o = up256(o + 4 * m);
+  p.off_colE = o;
+  o = up256(o + 4 * n);
+  p.off_flags = o; /* m row flags then n column flags, one byte each */
+  o = up256(o + m + n);
+  p.off_cnt = o;
+  o = up256(o + 16);
+  p.off_asl = o;
+  o = up256(o + (size_t)p.nprod * p.S * m * p.kp);
+  p.off_bsl = o;
+  o = up256(o + (size_t)p.nprod * p.S * n * p.kp);
+  p.off_d = o;
+  o = up256(o + (size_t)p.nprod * p.P * (2 * p.S - 1) * m * n * 4);
+  p.total = o;
+  return true;
+}
+
+/* element idx of a real (CPLX=false) or complex tiled matrix */
+template <int N, bool CPLX>
+__device__ __forceinline__ void load_any(fval<N> &re, fval<N> &im, const uint8_t *base, size_t idx) {
+  if (CPLX)
+    load_celem<N>(re, im, base, idx);
+  else
+    load_elem<N>(re, base, idx);
+}
+/* head word of element idx, part 0 (real / re) or 1 (im) */
+template <int N, bool CPLX>
+__device__ __forceinline__ uint32_t head_of(const uint8_t *base, size_t idx, int part) {
+  constexpr size_t TB = sol<N>::kTileBytes;
+  const uint8_t *t = base + (idx >> 5) * (CPLX ? 2u : 1u) * TB + (size_t)part * TB;
+  return __ldg((const uint32_t *)(t + sol<N>::kHeadOff) + (idx & 31u));
+}
+
+/* ------------------------------------------------------------------ *
+ * 1. exponent statistics
+ * ------------------------------------------------------------------ */
+/* one warp per row of A: E_i = max exponent of the nonzero entries (both
+ * parts of a complex entry); flag the row when some nonzero entry lies more
+ * than SP bits below E_i */
+template <int N, bool CPLX>
+__global__ void __launch_bounds__(256) k_row_stats(int m, int k, const uint8_t *A, size_t lda, int SP, int32_t *rowE,
+                                                   uint8_t *rowF, int *count) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= m) return;
+  int32_t emax = kExpZero, emin = 0x7fffffff;
+  for (int k0 = 0; k0 < k; k0 += 32) {
+    const int kk = k0 + lane;
+    if (kk < k) {
+#pragma unroll
+      for (int part = 0; part < (CPLX ? 2 : 1); ++part) {
+        const uint32_t h = head_of<N, CPLX>(A, (size_t)warp * lda + kk, part);
+        if (h != kHeadZero) {
+          const int32_t e = head_exp(h);
+          emax = max(emax, e);
+          emin = min(emin, e);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    emax = max(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+    emin = min(emin, __shfl_xor_sync(0xffffffffu, emin, o));
+  }
+  if (lane == 0) {
+    rowE[warp] = emax;
+    const bool flag = emax != kExpZero && (long)emax - emin > SP;
+    rowF[warp] = flag ? 1 : 0;
+    if (flag) atomicAdd(count, 1);
+  }
+}
+/* column statistics of B (k x n): block = 32 columns x 8 row groups */
+template <int N, bool CPLX>
+__global__ void __launch_bounds__(256) k_col_stats(int n, int k, const uint8_t *B, size_t ldb, int SP, int32_t *colE,
+                                                   uint8_t *colF, int *count) {
+  __shared__ int32_t smax[8][32], smin[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int j = blockIdx.x * 32 + lane;
+  int32_t emax = kExpZero, emin = 0x7fffffff;
+  for (int kk = w; kk < k; kk += 8) {
+#pragma unroll
+    for (int part = 0; part < (CPLX ? 2 : 1); ++part) {
+      const uint32_t h = head_of<N, CPLX>(B, (size_t)kk * ldb + j, part);
+      if (h != kHeadZero) {
+        const int32_t e = head_exp(h);
+        emax = max(emax, e);
+        emin = min(emin, e);
+      }
+    }
+  }
+  smax[w][lane] = emax;
+  smin[w][lane] = emin;
+  __syncthreads();
+  if (w == 0) {
+    for (int q = 1; q < 8; ++q) {
+      emax = max(emax, smax[q][lane]);
+      emin = min(emin, smin[q][lane]);
+    }
+    if (j < n) {
+      colE[j] = emax;
+      const bool flag = emax != kExpZero && (long)emax - emin > SP;
+      colF[j] = flag ? 1 : 0;
+      if (flag) atomicAdd(count, 1);
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ *
+ * 2. slicing into balanced base-256 digits
+ * ------------------------------------------------------------------ */
+/* V = (-1)^s * M * 2^sh, 0 <= sh = SP - (Erow - e) <= SP, as a two's
+ * complement integer of L+1 limbs (L = N + XL holds M << sh). */
+template <int N, int XL>
+__device__ __forceinline__ void aligned_twos(uint32_t (&w)[N + XL + 1], const fval<N> &x, int32_t Erow, int SP) {
+  constexpr int L = N + XL;
+  const bool zero = is_zero(x);
+  const uint32_t sh = zero ? 0u : (uint32_t)(SP - (Erow - x.e));
+  const uint32_t q = sh >> 5, r = sh & 31u;
+#pragma unroll
+  for (int i = 0; i <= L; ++i) w[i] = (i < N && !zero) ? x.m[i] : 0u;
+#pragma unroll
+  for (int b = 0; (1 << b) <= XL; ++b) { /* limb shift q < XL + 1 */
+    const int s = 1 << b;
+    const bool on = (q >> b) & 1u;
+#pragma unroll
+    for (int i = L; i >= 0; --i) {
+      const uint32_t src = (i - s >= 0) ? w[i - s] : 0u;
+      w[i] = on ? src : w[i];
+    }
+  }
+#pragma unroll
+  for (int i = L; i > 0; --i) w[i] = fshl(w[i - 1], w[i], r);
+  w[0] <<= r;
+  if (x.s && !zero) { /* negate */
+    uint32_t c = 1u;
+#pragma unroll
+    for (int i = 0; i <= L; ++i) {
+      const uint32_t t = ~w[i] + c;
+      c = (c && t == 0u) ? 1u : 0u;
+      w[i] = t;
+    }
+  }
+}
+/* balanced base-256 digits of a two's complement integer: byte b plus the
+ * incoming carry t becomes t - 256 (carry 1) when t >= 128.  For
+ * |V| < 2^(8S-2) every digit above S-1 is zero, so put(s, d) is called for
+ * s < S only. */
+template <int L1, typename F>
+__device__ __forceinline__ void twos_digits(const uint32_t (&w)[L1], int S, F put) {
+  uint32_t carry = 0;
+#pragma unroll
+  for (int s = 0; s < 4 * L1; ++s) {
+    const uint32_t t = ((w[s >> 2] >> (8 * (s & 3))) & 0xffu) + carry;
+    carry = (t >= 128u) ? 1u : 0u;
+    if (s < S) put(s, (int8_t)(carry ? (int)t - 256 : (int)t));
+  }
+}
+/* the digit stream of one element for product q: 0 (real / re part),
+ * 1 (im), 2 (re + im) */
+template <int N, int XL, bool CPLX, typename F>
+__device__ __forceinline__ void element_digits(const fval<N> &re, const fval<N> &im, int32_t E, int SP, int S,
+                                               int q, F put) {
+  uint32_t w[N + XL + 1];
+  aligned_twos<N, XL>(w, q == 1 ? im : re, E, SP);
+  if (CPLX && q == 2) {
+    uint32_t v[N + XL + 1];
+    aligned_twos<N, XL>(v, im, E, SP);
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i <= N + XL; ++i) {
+      const uint64_t t = (uint64_t)w[i] + v[i] + c;
+      w[i] = (uint32_t)t;
+      c = (uint32_t)(t >> 32);
+    }
+  }
+  twos_digits(w, S, put);
+}
+
+/* A (m x k, tiles) -> A_sl[q*S+s][i][kp]; thread per (i, kk), kk < kp (zero padding) */
+template <int N, int XL, bool CPLX>
+__global__ void __launch_bounds__(128) k_slice_a(int m, int k, int kp, const uint8_t *A, size_t lda, int SP, int S,
+                                                 const int32_t *rowE, const uint8_t *rowF, int8_t *Asl) {
+  const size_t total = (size_t)m * kp, plane = (size_t)m * kp;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / kp), kk = (int)(idx % kp);
+    fval<N> re, im;
+    set_zero(im);
+    if (kk < k && !rowF[i])
+      load_any<N, CPLX>(re, im, A, (size_t)i * lda + kk);
+    else
+      set_zero(re);
+    const int32_t E = rowE[i];
+    int8_t *dst = Asl + (size_t)i * kp + kk;
+#pragma unroll 1
+    for (int q = 0; q < (CPLX ? 3 : 1); ++q) {
+      int8_t *dq = dst + (size_t)q * S * plane;
+      element_digits<N, XL, CPLX>(re, im, E, SP, S, q, [&](int s, int8_t d) { dq[(size_t)s * plane] = d; });
+    }
+  }
+}
+
+/* B (k x n, tiles) -> B_sl[q*S+s][j][kp], transposed through shared memory:
+ * block = 32 columns (one tile) x 32 rows of B; digits staged per 32-plane
+ * chunk as [s][j][32 bytes of k], written out as 32-byte row segments. */
+template <int N, int XL, bool CPLX>
+__global__ void __launch_bounds__(256) k_slice_b(int n, int k, int kp, const uint8_t *B, size_t ldb, int SP, int S,
+                                                 const int32_t *colE, const uint8_t *colF, int8_t *Bsl) {
+  constexpr int CH = 32; /* digit planes per chunk */
+  __shared__ __align__(16) int8_t st[CH][32][32 + 16];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  const int j = j0 + lane;
+  const size_t plane = (size_t)n * kp;
+  fval<N> xr[4], xi[4];
+  const int32_t E = (j < n) ? colE[j] : kExpZero;
+  const bool skip = (j >= n) || colF[j];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int kk = k0 + w + 8 * r;
+    set_zero(xi[r]);
+    if (kk < k && !skip)
+      load_any<N, CPLX>(xr[r], xi[r], B, (size_t)kk * ldb + j);
+    else
+      set_zero(xr[r]);
+  }
+#pragma unroll 1
+  for (int q = 0; q < (CPLX ? 3 : 1); ++q) {
+    for (int c0 = 0; c0 < S; c0 += CH) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int kl = w + 8 * r;
+        element_digits<N, XL, CPLX>(xr[r], xi[r], E, SP, S, q, [&](int s, int8_t d) {
+          if (s >= c0 && s < c0 + CH) st[s - c0][lane][kl] = d;
+        });
+      }
+      __syncthreads();
+      /* write: for each plane s and column jl, 32 bytes of k (two uint4) */
+      const int nplanes = min(CH, S - c0);
+      for (int t = threadIdx.x; t < nplanes * 32 * 2; t += blockDim.x) {
+        const int half = t & 1, jl = (t >> 1) & 31, s = t >> 6;
+        if (j0 + jl < n) {
+          const uint4 v = *(const uint4 *)&st[s][jl][16 * half];
+          *(uint4 *)(Bsl + (size_t)(q * S + c0 + s) * plane + (size_t)(j0 + jl) * kp + k0 + 16 * half) = v;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ *
+ * 3. the tcgen05 diagonal GEMM
+ * ------------------------------------------------------------------ */
+struct GemmArgs {
+  int S, nprod, mt, nt, P, cpp, KC, m, n;
+  long units;
+  int32_t *D; /* [nprod][P][2S-1][m][n] */
+  int *err;
+};
+
+/* tensor-core phase (exact_gemm.cu): TMA maps over the digit planes and the
+ * persistent tcgen05 diagonal-GEMM launch; returns an mpb_status */
+int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *err, cudaStream_t st);
+
+/* ------------------------------------------------------------------ *
+ * 4. exact recombination and the single rounding
+ * ------------------------------------------------------------------ */
+/* Q 32-bit words cover sum_d 256^d D_d (2S-1 diagonals, up to 3 products
+ * with coefficients +-1 and 16 parts): 8(2S-2) + 31 + 8 + sign bits */
+template <int N, int XL>
+struct round_geo {
+  static constexpr int SMAX = 4 * (N + XL);
+  static constexpr int Q = (8 * (2 * SMAX - 2) + 31 + 8 + 31) / 32 + 1;
+};
+
+/* Normalise and round once: v[0..W) is the two's complement integer
+ * (LSB weight 2^lsb_exp) of an exact sum; r = RNDN(v) to N limbs. */
+template <int N, int W>
+__device__ __forceinline__ void round_words(fval<N> &r, uint32_t (&v)[W], long lsb_exp) {
+  const uint32_t neg = v[W - 1] >> 31;
+  if (neg) {
+    uint32_t c = 1;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      const uint32_t t = ~v[w] + c;
+      c = (c && t == 0) ? 1u : 0u;
+      v[w] = t;
+    }
+  }
+  int lq = W;
+  uint32_t top = 0;
+#pragma unroll
+  for (int w = W - 1; w >= 0; --w) {
+    const bool take = (lq == W) && v[w] != 0;
+    top = take ? v[w] : top;
+    lq = take ? (W - 1 - w) : lq;
+  }
+  if (lq == W) {
+    set_zero(r);
+    return;
+  }
+  const uint32_t lr = clz32(top) & 31u;
+#pragma unroll
+  for (int b = 0; (1 << b) < W; ++b) {
+    const int s = 1 << b;
+    const bool on = (lq >> b) & 1;
+#pragma unroll
+    for (int w = W - 1; w >= 0; --w) {
+      const uint32_t src = (w - s >= 0) ? v[w - s] : 0u;
+      v[w] = on ? src : v[w];
+    }
+  }
+#pragma unroll
+  for (int w = W - 1; w > 0; --w) v[w] = fshl(v[w - 1], v[w], lr);
+  v[0] <<= lr;
+#pragma unroll
+  for (int w = 0; w < N; ++w) r.m[w] = v[W - N + w];
+  const uint32_t g = v[W - N - 1];
+  uint32_t st = g << 1;
+#pragma unroll
+  for (int w = 0; w < W - N - 1; ++w) st |= v[w];
+  /* msb of the exact integer: 32*W - 1 - (32*lq + lr) */
+  const long msb = 32L * W - 1 - (32L * lq + lr);
+  int32_t ee = (int32_t)(msb + 1 + lsb_exp);
+  rndn<N>(r.m, ee, g >> 31, st);
+  r.e = ee;
+  r.s = neg;
+}
+
+/* Single k-part (P == 1): the diagonal planes of output idx are streamed
+ * word by word -- word w gathers diagonals 4w..4w+3 (each < 2^31, times
+ * 2^(8j) < 2^24) plus the carry of word w-1, keeps its low 32 bits and
+ * carries the rest on, so no wide accumulator is held.  Complex outputs read
+ * each product's plane once and form both components: re = T0 - T1,
+ * im = T2 - T0 - T1.  Every loop is unrolled at compile time. */
+template <int N, int XL, bool CPLX>
+__global__ void __launch_bounds__(128) k_exact_round(int m, int n, int S, int SP, const int32_t *D,
+                                                     const int32_t *rowE, const int32_t *colE, const uint8_t *rowF,
+                                                     const uint8_t *colF, uint8_t *C, size_t ldc) {
+  constexpr int Q = round_geo<N, XL>::Q;
+  constexpr int DMAX = 2 * round_geo<N, XL>::SMAX - 1;
+  const size_t total = (size_t)m * n, plane = (size_t)m * n;
+  const int ndiag = 2 * S - 1;
+  const size_t qstride = (size_t)ndiag * plane;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / n), j = (int)(idx % n);
+    if (rowF[i] || colF[j]) continue; /* computed by the fallback */
+    const long lsb = (long)rowE[i] + colE[j] - 2L * (32 * N) - 2L * SP;
+    uint32_t vr[Q], vi[CPLX ? Q : 1];
+    long long cr = 0, ci = 0;
+    const int32_t *d0 = D + idx;
+#pragma unroll
+    for (int w = 0; w < Q; ++w) {
+      long long tr = cr, ti = ci;
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const int d = 4 * w + jj;
+        if (d < DMAX && d < ndiag) {
+          const long long scale = 1LL << (8 * jj);
+          const long long t0 = __ldcs(d0 + (size_t)d * plane);
+          if (CPLX) {
+            const long long t1 = __ldcs(d0 + qstride + (size_t)d * plane);
+            const long long t2 = __ldcs(d0 + 2 * qstride + (size_t)d * plane);
+            tr += (t0 - t1) * scale;
+            ti += (t2 - t0 - t1) * scale;
+          } else {
+            tr += t0 * scale;
+          }
+        }
+      }
+      vr[w] = (uint32_t)tr;
+      cr = tr >> 32;
+      if (CPLX) {
+        vi[w] = (uint32_t)ti;
+        ci = ti >> 32;
+      }
+    }
+    fval<N> re;
+    round_words<N, Q>(re, vr, lsb);
+    if (CPLX) {
+      fval<N> im;
+      round_words<N, Q>(im, *reinterpret_cast<uint32_t(*)[Q]>(vi), lsb);
+      store_celem<N>(C, (size_t)i * ldc + j, re, im);
+    } else {
+      store_elem<N>(C, (size_t)i * ldc + j, re);
+    }
+  }
+}
+
+/* Several k-parts (P > 1, long k): the same sum with the parts added first.
+ * Written with run-time loops over per-thread local words to keep the code
+ * small; this path only serves k beyond 2^17/S. */
+template <int N, int XL, bool CPLX>
+__global__ void __launch_bounds__(128) k_exact_round_parts(int m, int n, int S, int SP, int P, const int32_t *D,
+                                                           const int32_t *rowE, const int32_t *colE,
+                                                           const uint8_t *rowF, const uint8_t *colF, uint8_t *C,
+                                                           size_t ldc) {
+  constexpr int Q = round_geo<N, XL>::Q;
+  const size_t total = (size_t)m * n, plane = (size_t)m * n;
+  const int ndiag = 2 * S - 1;
+  const size_t pstride = (size_t)ndiag * plane, qstride = (size_t)P * pstride;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / n), j = (int)(idx % n);
+    if (rowF[i] || colF[j]) continue;
+    const long lsb = (long)rowE[i] + colE[j] - 2L * (32 * N) - 2L * SP;
+#pragma unroll 1
+    for (int comp = 0; comp < (CPLX ? 2 : 1); ++comp) {
+      /* coefficients of T0, T1, T2 for this component */
+      const int c0 = CPLX ? (comp == 0 ? 1 : -1) : 1;
+      const int c1 = CPLX ? -1 : 0;
+      const int c2 = (CPLX && comp == 1) ? 1 : 0;
+      long long acc[Q];
+      for (int w = 0; w < Q; ++w) acc[w] = 0;
+#pragma unroll 1
+      for (int d = 0; d < ndiag; ++d) {
+        long long s = 0;
+#pragma unroll 1
+        for (int p = 0; p < P; ++p) {
+          const int32_t *dp = D + (size_t)p * pstride + (size_t)d * plane + idx;
+          s += (long long)c0 * __ldcs(dp);
+          if (c1) s += (long long)c1 * __ldcs(dp + qstride);
+          if (c2) s += (long long)c2 * __ldcs(dp + 2 * qstride);
+        }
+        acc[d >> 2] += s * (1LL << (8 * (d & 3)));
+      }
+      uint32_t v[Q];
+      long long carry = 0;
+#pragma unroll
+      for (int w = 0; w < Q; ++w) {
+        const long long t = acc[w] + carry;
+        v[w] = (uint32_t)t;
+        carry = t >> 32;
+      }
+      fval<N> r;
+      round_words<N, Q>(r, v, lsb);
+      const size_t e = (size_t)i * ldc + j;
+      if (CPLX) {
+        uint8_t *ct = C + (e >> 5) * 2u * sol<N>::kTileBytes + (size_t)comp * sol<N>::kTileBytes;
+        store_elem<N>(ct, e & 31u, r);
+      } else {
+        store_elem<N>(C, e, r);
+      }
+    }
+  }
+}
+
+/* flagged rows / columns: plain sequential-k per-operation rounding */
+template <int N, bool CPLX>
+__global__ void __launch_bounds__(256) k_fallback(size_t m, size_t n, size_t K, const uint8_t *A, size_t lda,
+                                                  const uint8_t *B, size_t ldb, uint8_t *C, size_t ldc,
+                                                  const uint8_t *rowF, const uint8_t *colF) {
+  const size_t i = (size_t)blockIdx.y * 8 + (threadIdx.x >> 5);
+  const size_t j = (size_t)blockIdx.x * 32u + (threadIdx.x & 31u);
+  if (i >= m || j >= n) return;
+  if (!rowF[i] && !colF[j]) return;
+  if (CPLX) {
+    fval<N> cr, ci;
+    set_zero(cr);
+    set_zero(ci);
+    for (size_t k = 0; k < K; ++k) {
+      fval<N> ar, ai, br, bi, tr, ti;
+      load_celem<N>(ar, ai, A, i * lda + k);
+      load_celem<N>(br, bi, B, k * ldb + j);
+      cmul<N, false>(tr, ti, br, bi, ar, ai);
+      add<N, false>(cr, cr, tr);
+      add<N, false>(ci, ci, ti);
+    }
+    store_celem<N>(C, i * ldc + j, cr, ci);
+  } else {
+    fval<N> acc;
+    set_zero(acc);
+    for (size_t k = 0; k < K; ++k) {
+      fval<N> a, b, t;
+      load_elem<N>(a, A, i * lda + k);
+      load_elem<N>(b, B, k * ldb + j);
+      mul<N>(t, b, a);
+      add<N, false>(acc, acc, t);
+    }
+    store_elem<N>(C, i * ldc + j, acc);
+  }
+}
+
+template <int N, int XL, bool CPLX>
+static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *B, size_t ldb, uint8_t *C,
+                    size_t ldc, uint8_t *ws, int *n_fallback, cudaStream_t st) {
+  int32_t *rowE = (int32_t *)(ws + p.off_rowE), *colE = (int32_t *)(ws + p.off_colE);
+  uint8_t *rowF = ws + p.off_flags, *colF = ws + p.off_flags + p.m;
+  int *cnt = (int *)(ws + p.off_cnt); /* [0] fallback rows+cols, [1] kernel error code */
+  int8_t *Asl = (int8_t *)(ws + p.off_asl), *Bsl = (int8_t *)(ws + p.off_bsl);
+  int32_t *D = (int32_t *)(ws + p.off_d);
+  if (cudaMemsetAsync(cnt, 0, 16, st) != cudaSuccess) return MPB_ERR_CUDA;
+
+  profile_mark(kPhaseStats, true, st);
+  k_row_stats<N, CPLX><<<(p.m + 7) / 8, 256, 0, st>>>(p.m, p.k, A, lda, p.SP, rowE, rowF, cnt);
+  k_col_stats<N, CPLX><<<(p.n + 31) / 32, 256, 0, st>>>(p.n, p.k, B, ldb, p.SP, colE, colF, cnt);
+  profile_mark(kPhaseStats, false, st);
+  profile_mark(kPhaseSlice, true, st);
+  {
+    const int g = grid_for(k_slice_a<N, XL, CPLX>, 128, (size_t)p.m * p.kp);
+    k_slice_a<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.k, p.kp, A, lda, p.SP, p.S, rowE, rowF, Asl);
+  }
+  {
+    const dim3 grid((p.n + 31) / 32, p.kp / 32);
+    k_slice_b<N, XL, CPLX><<<grid, 256, 0, st>>>(p.n, p.k, p.kp, B, ldb, p.SP, p.S, colE, colF, Bsl);
+  }
+  profile_mark(kPhaseSlice, false, st);
+  if (launch_status() != MPB_OK) return MPB_ERR_CUDA;
+
+  {
+    const int rc = launch_diag_gemm(p, Asl, Bsl, D, cnt + 1, st);
+    if (rc != MPB_OK) return rc;
+  }
+
+  profile_mark(kPhaseRound, true, st);
+  if (p.P == 1) {
+    const int g = grid_for(k_exact_round<N, XL, CPLX>, 128, (size_t)p.m * p.n);
+    k_exact_round<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.n, p.S, p.SP, D, rowE, colE, rowF, colF, C, ldc);
+  } else {
+    const int g = grid_for(k_exact_round_parts<N, XL, CPLX>, 128, (size_t)p.m * p.n);
+    k_exact_round_parts<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.n, p.S, p.SP, p.P, D, rowE, colE, rowF, colF, C,
+                                                        ldc);
+  }
+  profile_mark(kPhaseRound, false, st);
+  profile_mark(kPhaseFallback, true, st);
+  {
+    const dim3 grid((p.n + 31) / 32, (p.m + 7) / 8);
+    k_fallback<N, CPLX><<<grid, 256, 0, st>>>(p.m, p.n, p.k, A, lda, B, ldb, C, ldc, rowF, colF);
+  }
+  profile_mark(kPhaseFallback, false, st);
+  if (n_fallback && cudaMemcpyAsync(n_fallback, cnt, 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return MPB_ERR_CUDA;
+  return launch_status();
+}
+
+template <int N, int XL>
+int run_exact(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *B, size_t ldb, uint8_t *C,
+                     size_t ldc, uint8_t *ws, int *n_fallback, cudaStream_t st) {
+  if (p.cplx) return run_impl<N, XL, true>(p, A, lda, B, ldb, C, ldc, ws, n_fallback, st);
+  return run_impl<N, XL, false>(p, A, lda, B, ldb, C, ldc, ws, n_fallback, st);
+}
+
+/* one precision, any spread budget (instantiated in exact_gemm_pb<32N>.cu) */
+template <int N>
+int run_exact_n(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *B, size_t ldb, uint8_t *C, size_t ldc,
+                uint8_t *ws, int *n_fallback, cudaStream_t st) {
+  switch (p.XL) {
+    case 1:
+      return run_exact<N, 1>(p, A, lda, B, ldb, C, ldc, ws, n_fallback, st);
+    case 2:
+      return run_exact<N, 2>(p, A, lda, B, ldb, C, ldc, ws, n_fallback, st);
+    case 4:
+      return run_exact<N, 4>(p, A, lda, B, ldb, C, ldc, ws, n_fallback, st);
+    default:
+      return MPB_ERR_ARG;
+  }
+}
+
+#define MPB_EXACT_DECLARE(N)                                                                                    \
+  extern template int run_exact_n<N>(const Plan &, const uint8_t *, size_t, const uint8_t *, size_t, uint8_t *, \
+                                     size_t, uint8_t *, int *, cudaStream_t);
+MPB_EXACT_DECLARE(2)
+MPB_EXACT_DECLARE(4)
+MPB_EXACT_DECLARE(8)
+MPB_EXACT_DECLARE(16)
+MPB_EXACT_DECLARE(32)
+MPB_EXACT_DECLARE(64)
+
+} /* namespace exact */
+} /* namespace mpb */
+
+#endif /* MPB_EXACT_GEMM_CUH */

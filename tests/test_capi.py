@@ -83,3 +83,13 @@ def test_exact_gemm_workspace_and_checks(mpb):
     assert L.mpb_gemm_exact_r(512, 8, 8, 8, good, 32, good, 32, good, 32, 32, good + 16, 1 << 30, None, None) == -4
     assert L.mpb_gemm_exact_r(512, 8, 8, 8, good, 40, good, 32, good, 32, 32, good, 1 << 30, None, None) == -5
     assert L.mpb_gemm_exact_r(512, 0, 8, 8, None, 32, None, 32, None, 32, 32, None, 0, None, None) == 0
+
+
+def test_exact_gemm_complex_workspace(mpb):
+    L = mpb.lib()
+    # PB=256, 512^3 complex, 16-bit spread: S = ceil((256+16+3)/8) = 35, 3 products
+    S, m = 35, 512
+    need = L.mpb_gemm_exact_c_workspace(256, m, m, m, 16)
+    planes = 3 * S * 2 * m * m + 3 * (2 * S - 1) * m * m * 4
+    assert planes <= need <= planes + 64 * 1024
+    assert L.mpb_gemm_exact_c(256, 8, 8, 8, 4096, 32, 4096, 32, 4096, 32, 16, None, 0, None, None) == -8

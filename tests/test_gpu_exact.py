@@ -119,3 +119,111 @@ def test_exact_real_pb512_full_size(orc, mpb):
         e4 = orc.gemm_exact(prec, m, n, k, A, k, B, n, out_prec=4 * prec, rows=(r0, r1))
         ulp = orc.ulp_errors(prec, got[sel], 4 * prec, e4[r0 * n * 1:r1 * n])
         assert ulp.max() <= 0.5
+
+
+def rand_caos(prec, count, seed, elo=-8, ehi=8, zero_frac=0.05):
+    rng = np.random.default_rng(seed)
+    re = synth.random_elems(rng, prec, count, elo, ehi, zero_frac)
+    im = synth.random_elems(rng, prec, count, elo, ehi, zero_frac)
+    return synth.interleave_complex(prec, re, im)
+
+
+def pad_rows_c(prec, A, rows, cols, ld):
+    z1 = layout.aos_from_parts(prec, np.zeros((1, prec // 32), np.uint32), np.array([layout.HEAD_ZERO], np.uint32))
+    z = np.concatenate([z1, z1], axis=1)
+    es = A.shape[1]
+    out = np.repeat(z, rows * ld, axis=0).reshape(rows, ld, es)
+    out[:, :cols] = A.reshape(rows, cols, es)
+    return out.reshape(rows * ld, es)
+
+
+def run_exact_c(mpb, prec, m, n, k, A, B, sp_bits):
+    import torch
+
+    lda, ldb, ldc = (-(-k // 32) * 32, -(-n // 32) * 32, -(-n // 32) * 32)
+    dA = to_dev(layout.aos_to_vec(prec, pad_rows_c(prec, A, m, k, lda), True))
+    dB = to_dev(layout.aos_to_vec(prec, pad_rows_c(prec, B, k, n, ldb), True))
+    Cd = mpb.empty(prec, m * ldc, True)
+    st = torch.zeros(2, dtype=torch.int32, device="cuda")
+    mpb.gemm_exact(prec, m, n, k, dA, lda, dB, ldb, Cd, ldc, sp_bits=sp_bits, status=st, cplx=True)
+    C = layout.vec_to_aos(prec, to_host(Cd), m * ldc, True).reshape(m, ldc, -1)[:, :n].reshape(m * n, -1)
+    return C, st.cpu().numpy()
+
+
+@pytest.mark.parametrize("prec", (64, 256, 512, 1024))
+@pytest.mark.parametrize("shape", ((1, 1, 1), (5, 7, 33), (33, 40, 17), (130, 260, 300)))
+def test_exact_complex_vs_mpc_dot(orc, mpb, prec, shape):
+    """Each component is one rounding of the exact complex dot (mpc_dot),
+    computed with three exact integer products (Gauss form)."""
+    m, n, k = shape
+    if prec == 1024 and m * n * k > 200000:
+        pytest.skip("covered at smaller shapes")
+    A = rand_caos(prec, m * k, 300 + m + prec)
+    B = rand_caos(prec, k * n, 400 + n + prec)
+    C, st = run_exact_c(mpb, prec, m, n, k, A, B, sp_bits=16)
+    assert st[1] == 0 and st[0] == 0
+    exp = orc.gemm_exact(prec, m, n, k, A, k, B, n, cplx=True, impl="mp")
+    bad, first = orc.mismatches(prec, C, exp, True)
+    assert bad == 0, f"PB={prec} {shape}: {bad} mismatches, first at {first}"
+
+
+def test_exact_complex_fallback(orc, mpb):
+    prec, m, n, k = 256, 12, 40, 30
+    A = rand_caos(prec, m * k, 41, -4, 4, 0.0).reshape(m, k, -1)
+    B = rand_caos(prec, k * n, 42, -4, 4, 0.0)
+    es = layout.aos_bytes(prec)
+    A[4, 2, es + 8:es + 16] = np.array([-500], np.int64).view(np.uint8)  # imaginary part far below
+    A = A.reshape(m * k, -1)
+    C, st = run_exact_c(mpb, prec, m, n, k, A, B, sp_bits=32)
+    assert st[1] == 0 and st[0] == 1
+    exact = orc.gemm_exact(prec, m, n, k, A, k, B, n, cplx=True, impl="mp").reshape(m, n, -1)
+    plain = orc.gemm(prec, m, n, k, A, k, B, n, cplx=True, impl="mp").reshape(m, n, -1)
+    C = C.reshape(m, n, -1)
+    assert orc.mismatches(prec, C[4], plain[4], True)[0] == 0
+    for i in (0, 3, 5, 11):
+        assert orc.mismatches(prec, C[i], exact[i], True)[0] == 0
+
+
+@pytest.mark.parametrize("cplx", (False, True))
+def test_exact_long_k_split_into_parts(orc, mpb, cplx):
+    """k beyond 2^17/S splits every diagonal into k-parts (separate int32
+    planes summed in the rounding): results must stay correctly rounded."""
+    prec, m, n, k = 512, 9, 33, 2400
+    if cplx:
+        A, B = rand_caos(prec, m * k, 51), rand_caos(prec, k * n, 52)
+        C, st = run_exact_c(mpb, prec, m, n, k, A, B, sp_bits=16)
+    else:
+        A, B = rand_aos(prec, m * k, 51), rand_aos(prec, k * n, 52)
+        C, st = run_exact(mpb, prec, m, n, k, A, B, sp_bits=16)
+    assert st[1] == 0 and st[0] == 0
+    exp = orc.gemm_exact(prec, m, n, k, A, k, B, n, cplx=cplx, impl="mp")
+    assert orc.mismatches(prec, C, exp, cplx)[0] == 0
+
+
+def test_exact_complex_pb256_full_size(orc, mpb):
+    """The 512^3 complex PB=256 workload: 8-limb entries, exponents in [-8, 8];
+    a row sample must equal mpc_dot and be <= 0.5 ULP per component from the
+    exact sum at 1024 bits."""
+    import torch
+
+    prec, m, n, k = 256, 512, 512, 512
+    (ar, ai), (br, bi) = synth.gemm_c256()
+    A, B = synth.interleave_complex(prec, ar, ai), synth.interleave_complex(prec, br, bi)
+    dA = to_dev(layout.aos_to_vec(prec, A, True))
+    dB = to_dev(layout.aos_to_vec(prec, B, True))
+    Cd = mpb.empty(prec, m * n, True)
+    st = torch.zeros(2, dtype=torch.int32, device="cuda")
+    mpb.gemm_exact(prec, m, n, k, dA, k, dB, n, Cd, n, sp_bits=16, status=st, cplx=True)
+    st = st.cpu().numpy()
+    assert st[1] == 0 and st[0] == 0
+    got = layout.vec_to_aos(prec, to_host(Cd), m * n, True)
+    for r0, r1 in ((0, 1), (300, 301), (m - 1, m)):
+        sel = slice(r0 * n, r1 * n)
+        exp = orc.gemm_exact(prec, m, n, k, A, k, B, n, cplx=True, impl="mp", rows=(r0, r1))
+        assert orc.mismatches(prec, got[sel], exp[sel], True)[0] == 0
+        e4 = orc.gemm_exact(prec, m, n, k, A, k, B, n, cplx=True, out_prec=4 * prec, rows=(r0, r1))
+        es, e4s = layout.aos_bytes(prec), layout.aos_bytes(4 * prec)
+        for part in (0, 1):
+            g = got[sel][:, part * es:(part + 1) * es]
+            w = e4[sel][:, part * e4s:(part + 1) * e4s]
+            assert orc.ulp_errors(prec, g, 4 * prec, w).max() <= 0.5
