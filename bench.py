@@ -295,7 +295,7 @@ class GemmWorkload:
 
     @property
     def default_steps(self):
-        return 200  # ~1 s of GPU time: long enough for clock sampling
+        return 2000 if self.cplx else 200  # ~1 s of GPU time: long enough for clock sampling
 
     launches_per_step = 7  # stats x2, slice x2, tensor-core GEMM, round, fallback
     e2e_launches_per_step = 10
