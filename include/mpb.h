@@ -113,6 +113,39 @@ int mpb_gemm_r(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda
 int mpb_gemm_c(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
                void *C, size_t ldc, void *stream);
 
+/* ---- batched GEMV: thousands of independent problems, mixed sizes and precisions ---- */
+/* One problem y_out = A.x + y (real, prec bits, same order as mpb_gemv_r).
+ * Device pointers; lda a multiple of 32 (>= n); m or n may be 0. */
+typedef struct {
+  int prec;
+  int m, n;
+  size_t lda;
+  const void *A, *x, *y;
+  void *y_out;
+} mpb_gemv_problem;
+typedef struct mpb_batch_plan mpb_batch_plan;
+/* Bytes of device workspace a plan for `count` problems needs (256-byte aligned). */
+size_t mpb_batch_gemv_workspace(int count);
+/* Validate the problems (host array), group them by precision, order each
+ * group longest first and upload descriptors and work queues to the
+ * workspace (synchronous); returns an opaque host-side plan.  The reference
+ * has no batched path (its matvec is tools/linalg_fast.cu:37-51). */
+int mpb_batch_gemv_plan(int count, const mpb_gemv_problem *problems, void *workspace, size_t ws_bytes,
+                        mpb_batch_plan **plan);
+/* Run every planned problem: one persistent kernel per precision present,
+ * forked onto the plan's streams and joined back into `stream`; no
+ * allocation, no host synchronisation (can be captured into a CUDA graph).
+ * Runs of one plan must not overlap (they share the workspace queues). */
+int mpb_batch_gemv_run(mpb_batch_plan *plan, void *stream);
+/* Time each precision group with every candidate launch shape on the planned
+ * batch (synchronous) and keep the fastest in the plan. */
+int mpb_batch_gemv_autotune(mpb_batch_plan *plan, void *stream);
+/* Read / install the launch shape of a precision group (threads per block, a
+ * multiple of 32 up to 256; persistent blocks per SM, 0 = occupancy limit). */
+int mpb_batch_gemv_get_tuning(const mpb_batch_plan *plan, int prec, int *block, int *blocks_per_sm);
+int mpb_batch_gemv_set_tuning(mpb_batch_plan *plan, int prec, int block, int blocks_per_sm);
+void mpb_batch_gemv_destroy(mpb_batch_plan *plan);
+
 /* ---- exact-accumulation GEMM on the INT8 tensor cores (no counterpart in the reference) ---- */
 /* C[i,j] = RNDN(sum_k A[i,k]*B[k,j]) with ONE rounding per entry: the correctly
  * rounded dot product (MPFR mpfr_dot semantics; <= 0.5 ULP).  Each row of A and

@@ -64,6 +64,13 @@ _SIGS = {
     "mpb_gemv_c": ([_I, _S, _S, _V, _S, _V, _V, _V, _V], C.c_int),
     "mpb_gemm_r": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _V], C.c_int),
     "mpb_gemm_c": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _V], C.c_int),
+    "mpb_batch_gemv_workspace": ([_I], C.c_size_t),
+    "mpb_batch_gemv_plan": ([_I, _V, _V, _S, C.POINTER(_V)], C.c_int),
+    "mpb_batch_gemv_run": ([_V, _V], C.c_int),
+    "mpb_batch_gemv_autotune": ([_V, _V], C.c_int),
+    "mpb_batch_gemv_get_tuning": ([_V, _I, C.POINTER(_I), C.POINTER(_I)], C.c_int),
+    "mpb_batch_gemv_set_tuning": ([_V, _I, _I, _I], C.c_int),
+    "mpb_batch_gemv_destroy": ([_V], None),
     "mpb_gemm_exact_workspace": ([_I, _S, _S, _S, _I], C.c_size_t),
     "mpb_profile_enable": ([_I], None),
     "mpb_profile_phase_ms": ([_I], C.c_float),
@@ -232,8 +239,67 @@ def gemm_exact(prec, m, n, k, A, lda, B, ldb, Cm, ldc, sp_bits=32, workspace=Non
     return workspace
 
 
+class GemvProblem(C.Structure):
+    """mpb_gemv_problem: y_out = A.x + y at precision prec (device pointers)."""
+    _fields_ = [("prec", C.c_int), ("m", C.c_int), ("n", C.c_int), ("lda", C.c_size_t), ("A", C.c_void_p),
+                ("x", C.c_void_p), ("y", C.c_void_p), ("y_out", C.c_void_p)]
+
+
+class BatchGemv:
+    """A planned batch of independent GEMV problems (mixed sizes and precisions).
+
+    ``problems``: iterable of (prec, m, n, lda, A, x, y, y_out) with torch CUDA
+    tensors (or raw device addresses).  ``run()`` launches every problem (no
+    host synchronisation, capturable in a CUDA graph); ``autotune()`` picks the
+    launch shape per precision on this batch; ``tuning``/``set_tuning`` read
+    and install cached choices."""
+
+    def __init__(self, problems, device="cuda"):
+        import torch
+
+        probs = [GemvProblem(p, m, n, lda, _ptr(A), _ptr(x), _ptr(y), _ptr(yo))
+                 for (p, m, n, lda, A, x, y, yo) in problems]
+        self.count = len(probs)
+        arr = (GemvProblem * self.count)(*probs)
+        nbytes = int(lib().mpb_batch_gemv_workspace(self.count))
+        self.workspace = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=device)
+        h = C.c_void_p()
+        _call("mpb_batch_gemv_plan", self.count, C.cast(arr, C.c_void_p), _ptr(self.workspace), nbytes, C.byref(h))
+        self._plan = h
+
+    def run(self, stream=None):
+        _call("mpb_batch_gemv_run", self._plan, _stream(stream))
+
+    def autotune(self, stream=None):
+        _call("mpb_batch_gemv_autotune", self._plan, _stream(stream))
+
+    def tuning(self):
+        out = {}
+        for p in SUPPORTED:
+            b, s = C.c_int(), C.c_int()
+            _call("mpb_batch_gemv_get_tuning", self._plan, p, C.byref(b), C.byref(s))
+            out[p] = (b.value, s.value)
+        return out
+
+    def set_tuning(self, table):
+        for p, (b, s) in table.items():
+            _call("mpb_batch_gemv_set_tuning", self._plan, int(p), int(b), int(s))
+
+    def close(self):
+        if getattr(self, "_plan", None):
+            lib().mpb_batch_gemv_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 __all__ = [
     "SUPPORTED", "MpbError", "aos_bytes", "tile_bytes", "vec_bytes", "build", "lib", "host_lib", "empty",
     "empty_matrix", "pack_aos", "unpack_aos", "from_double", "to_double", "binop", "fma", "axpy", "gemv", "gemm",
-    "layout", "MPB_OP_MUL", "MPB_OP_ADD", "MPB_OP_SUB", "gemm_exact", "gemm_exact_workspace",
+    "layout", "MPB_OP_MUL", "MPB_OP_ADD", "MPB_OP_SUB", "gemm_exact", "gemm_exact_workspace", "BatchGemv",
+    "GemvProblem",
 ]

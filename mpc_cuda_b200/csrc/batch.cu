@@ -1,0 +1,347 @@
+/* batch.cu -- thousands of independent GEMV problems y_out = A.x + y of uneven
+ * sizes and mixed precisions in one launch sequence.
+ *
+ * Every problem keeps the per-operation-rounded, sequential-k order of
+ * mpb_gemv_r (acc = +0; acc = round(acc + round(A[i,k] x[k])); y_out[i] =
+ * round(acc + y[i])), so each result is bit-exact with MPFR at its own
+ * precision.
+ *
+ * plan (host, once): validate every descriptor, group the problems by
+ * precision, order each group by decreasing cost (n * N^2 per row), split
+ * them into 32-row units (one warp each) and upload the descriptors, the
+ * problem order and each group's unit prefix sums into the caller's
+ * workspace.  run (device, any number of times): reset the queue counters,
+ * fork one persistent kernel per precision present onto auxiliary streams,
+ * join them back.  Warps claim units from the group's atomic queue, longest
+ * problems first, so the uneven batch balances itself.  run allocates
+ * nothing and never synchronises the host, so the whole call can be
+ * captured into a CUDA graph by the caller.  autotune times each group with
+ * every candidate (block size, blocks per SM) on the planned batch and keeps
+ * the fastest; set_tuning installs a cached choice.
+ */
+#include <algorithm>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mpb {
+namespace batch {
+
+constexpr int kGroups = 6; /* 64, 128, 256, 512, 1024, 2048 */
+inline int group_of(int prec) {
+  switch (prec) {
+    case 64: return 0;
+    case 128: return 1;
+    case 256: return 2;
+    case 512: return 3;
+    case 1024: return 4;
+    case 2048: return 5;
+    default: return -1;
+  }
+}
+
+struct DevProb { /* device copy of one problem */
+  const uint8_t *A, *x, *y;
+  uint8_t *yo;
+  int m, n;
+  long long lda;
+};
+
+struct Tuning {
+  int block;        /* threads per block (multiple of 32) */
+  int blocks_per_sm; /* persistent grid: SMs x this (capped by occupancy) */
+};
+
+/* candidates tried by the autotuner */
+static const Tuning kCandidates[] = {{64, 2}, {64, 4}, {128, 1}, {128, 2}, {128, 4}, {256, 1}, {256, 2}};
+
+template <int N>
+__global__ void __launch_bounds__(256) k_batch_gemv(const DevProb *probs, const int *order, const long long *prefix,
+                                                    int nprob, long long nunits, unsigned long long *counter) {
+  const int lane = threadIdx.x & 31;
+  while (true) {
+    long long u = 0;
+    if (lane == 0) u = (long long)atomicAdd(counter, 1ull);
+    u = __shfl_sync(0xffffffffu, u, 0);
+    if (u >= nunits) break;
+    /* problem owning unit u: last p with prefix[p] <= u */
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prefix[mid] <= u)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const DevProb pr = probs[order[lo]];
+    const long long blk = u - prefix[lo];
+    const int i = (int)(blk * 32) + lane;
+    const int ir = i < pr.m ? i : pr.m - 1; /* padding lanes recompute the last row */
+    fval<N> acc, yv;
+    set_zero(acc);
+    const uint8_t *arow = pr.A;
+    for (int k = 0; k < pr.n; ++k) {
+      fval<N> a, xv, t;
+      load_elem<N>(a, arow, (size_t)ir * pr.lda + k);
+      load_elem<N>(xv, pr.x, k);
+      mul<N>(t, a, xv);
+      add<N, true>(acc, acc, t);
+    }
+    load_elem<N>(yv, pr.y, ir);
+    add<N, true>(acc, acc, yv);
+    if (i < pr.m) store_elem<N>(pr.yo, i, acc);
+  }
+}
+
+using KernelFn = void (*)(const DevProb *, const int *, const long long *, int, long long, unsigned long long *);
+static KernelFn kernel_of(int g) {
+  switch (g) {
+    case 0: return k_batch_gemv<2>;
+    case 1: return k_batch_gemv<4>;
+    case 2: return k_batch_gemv<8>;
+    case 3: return k_batch_gemv<16>;
+    case 4: return k_batch_gemv<32>;
+    default: return k_batch_gemv<64>;
+  }
+}
+
+} /* namespace batch */
+} /* namespace mpb */
+
+using namespace mpb;
+using namespace mpb::batch;
+
+/* opaque host-side plan */
+struct mpb_batch_plan {
+  int device;
+  int count;
+  uint8_t *ws;
+  DevProb *probs;   /* device */
+  int *order;       /* device: problem indices, grouped, longest first */
+  long long *prefix; /* device: per-group unit prefix sums */
+  int *counters;    /* device: one queue counter per group */
+  int gstart[kGroups], gcount[kGroups];
+  long long gunits[kGroups];
+  double gwork[kGroups]; /* relative cost of each group */
+  Tuning tune[kGroups];
+  cudaStream_t aux[kGroups];
+  cudaEvent_t fork, join[kGroups];
+};
+
+static size_t up256b(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static void layout_ws(int count, size_t *o_probs, size_t *o_order, size_t *o_prefix, size_t *o_cnt, size_t *total) {
+  size_t o = 0;
+  *o_probs = o;
+  o = up256b(o + sizeof(DevProb) * (size_t)count);
+  *o_order = o;
+  o = up256b(o + sizeof(int) * (size_t)count);
+  *o_prefix = o;
+  o = up256b(o + sizeof(long long) * (size_t)(count + kGroups));
+  *o_cnt = o;
+  o = up256b(o + 64 * kGroups);
+  *total = o;
+}
+
+extern "C" size_t mpb_batch_gemv_workspace(int count) {
+  if (count <= 0 || count > (1 << 24)) return 0;
+  size_t a, b, c, d, t;
+  layout_ws(count, &a, &b, &c, &d, &t);
+  return t;
+}
+
+static int check_prob(const mpb_gemv_problem &p) {
+  const int g = group_of(p.prec);
+  if (g < 0) return MPB_ERR_PREC;
+  if (p.m < 0 || p.n < 0 || p.m > (1 << 24) || p.n > (1 << 24)) return MPB_ERR_SIZE;
+  if (p.m == 0) return MPB_OK;
+  if (p.n > 0 && (p.lda % 32 != 0 || p.lda < (size_t)p.n)) return MPB_ERR_LD;
+  if (!p.y || !p.y_out || (p.n > 0 && (!p.A || !p.x))) return MPB_ERR_NULL;
+  if (!aligned16(p.y) || !aligned16(p.y_out) || (p.n > 0 && (!aligned16(p.A) || !aligned16(p.x))))
+    return MPB_ERR_ALIGN;
+  return MPB_OK;
+}
+
+extern "C" int mpb_batch_gemv_plan(int count, const mpb_gemv_problem *problems, void *workspace, size_t ws_bytes,
+                                   mpb_batch_plan **plan_out) {
+  if (!plan_out) return MPB_ERR_NULL;
+  *plan_out = nullptr;
+  if (count <= 0 || count > (1 << 24)) return MPB_ERR_SIZE;
+  if (!problems) return MPB_ERR_NULL;
+  size_t o_probs, o_order, o_prefix, o_cnt, total;
+  layout_ws(count, &o_probs, &o_order, &o_prefix, &o_cnt, &total);
+  if (!workspace || ws_bytes < total) return MPB_ERR_WORKSPACE;
+  if (((uintptr_t)workspace & 255u) != 0) return MPB_ERR_ALIGN;
+  for (int i = 0; i < count; ++i) {
+    const int rc = check_prob(problems[i]);
+    if (rc != MPB_OK) return rc;
+  }
+  /* group by precision, longest (per-row cost) first */
+  std::vector<int> idx(count);
+  for (int i = 0; i < count; ++i) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+    const int ga = group_of(problems[a].prec), gb = group_of(problems[b].prec);
+    if (ga != gb) return ga < gb;
+    return problems[a].n > problems[b].n;
+  });
+  mpb_batch_plan *pl = new (std::nothrow) mpb_batch_plan();
+  if (!pl) return MPB_ERR_ARG;
+  if (cudaGetDevice(&pl->device) != cudaSuccess) {
+    delete pl;
+    return MPB_ERR_CUDA;
+  }
+  pl->count = count;
+  pl->ws = (uint8_t *)workspace;
+  pl->probs = (DevProb *)(pl->ws + o_probs);
+  pl->order = (int *)(pl->ws + o_order);
+  pl->prefix = (long long *)(pl->ws + o_prefix);
+  pl->counters = (int *)(pl->ws + o_cnt);
+  std::vector<DevProb> hp(count);
+  std::vector<long long> pre(count + kGroups, 0);
+  for (int g = 0; g < kGroups; ++g) {
+    pl->gstart[g] = 0;
+    pl->gcount[g] = 0;
+    pl->gunits[g] = 0;
+    pl->gwork[g] = 0.0;
+    pl->tune[g] = Tuning{128, 0}; /* 0: full occupancy */
+  }
+  for (int i = 0; i < count; ++i) {
+    const mpb_gemv_problem &p = problems[i];
+    hp[i] = DevProb{(const uint8_t *)p.A, (const uint8_t *)p.x, (const uint8_t *)p.y, (uint8_t *)p.y_out,
+                    p.m, p.n, (long long)p.lda};
+  }
+  /* per group: order slice and unit prefix sums (prefix array holds, for each
+   * group, its problems' prefixes contiguously at [gstart, gstart+gcount)) */
+  int pos = 0;
+  for (int g = 0; g < kGroups; ++g) {
+    pl->gstart[g] = pos;
+    long long units = 0;
+    while (pos < count && group_of(problems[idx[pos]].prec) == g) {
+      const mpb_gemv_problem &p = problems[idx[pos]];
+      pre[pos] = units;
+      units += (p.m + 31) / 32;
+      const double N = p.prec / 32.0;
+      pl->gwork[g] += (double)p.m * p.n * N * N;
+      ++pos;
+    }
+    pl->gcount[g] = pos - pl->gstart[g];
+    pl->gunits[g] = units;
+  }
+  bool ok = cudaMemcpy(pl->probs, hp.data(), sizeof(DevProb) * count, cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(pl->order, idx.data(), sizeof(int) * count, cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(pl->prefix, pre.data(), sizeof(long long) * count, cudaMemcpyHostToDevice) == cudaSuccess;
+  for (int g = 0; g < kGroups && ok; ++g) {
+    ok = cudaStreamCreateWithFlags(&pl->aux[g], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&pl->join[g], cudaEventDisableTiming) == cudaSuccess;
+  }
+  ok = ok && cudaEventCreateWithFlags(&pl->fork, cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    mpb_batch_gemv_destroy(pl);
+    return MPB_ERR_CUDA;
+  }
+  *plan_out = pl;
+  return MPB_OK;
+}
+
+static int launch_group(mpb_batch_plan *pl, int g, cudaStream_t st, double share) {
+  if (pl->gcount[g] == 0 || pl->gunits[g] == 0) return MPB_OK;
+  KernelFn fn = kernel_of(g);
+  const Tuning t = pl->tune[g];
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, t.block, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const int bps = t.blocks_per_sm > 0 ? std::min(t.blocks_per_sm, per_sm) : per_sm;
+  long long grid = (long long)std::max(1.0, share * sm_count() * bps + 0.5);
+  const long long warps_needed = pl->gunits[g];
+  const long long max_grid = (warps_needed * 32 + t.block - 1) / t.block;
+  grid = std::min(grid, std::max(1LL, max_grid));
+  fn<<<(int)grid, t.block, 0, st>>>(pl->probs, pl->order + pl->gstart[g], pl->prefix + pl->gstart[g], pl->gcount[g],
+                                    pl->gunits[g], (unsigned long long *)((uint8_t *)pl->counters + 64 * g));
+  return launch_status();
+}
+
+extern "C" int mpb_batch_gemv_run(mpb_batch_plan *pl, void *stream) {
+  if (!pl) return MPB_ERR_NULL;
+  cudaStream_t st = as_stream(stream);
+  if (cudaMemsetAsync(pl->counters, 0, 64 * kGroups, st) != cudaSuccess) return MPB_ERR_CUDA;
+  double total = 0.0;
+  for (int g = 0; g < kGroups; ++g) total += pl->gwork[g];
+  if (total <= 0.0) return MPB_OK;
+  if (cudaEventRecord(pl->fork, st) != cudaSuccess) return MPB_ERR_CUDA;
+  int rc = MPB_OK;
+  for (int g = 0; g < kGroups; ++g) {
+    if (pl->gcount[g] == 0) continue;
+    if (cudaStreamWaitEvent(pl->aux[g], pl->fork, 0) != cudaSuccess) return MPB_ERR_CUDA;
+    /* each group gets the share of the GPU its work needs, so all finish together */
+    const int r = launch_group(pl, g, pl->aux[g], pl->gwork[g] / total);
+    if (r != MPB_OK) rc = r;
+    if (cudaEventRecord(pl->join[g], pl->aux[g]) != cudaSuccess || cudaStreamWaitEvent(st, pl->join[g], 0) != cudaSuccess)
+      return MPB_ERR_CUDA;
+  }
+  return rc;
+}
+
+extern "C" int mpb_batch_gemv_autotune(mpb_batch_plan *pl, void *stream) {
+  if (!pl) return MPB_ERR_NULL;
+  cudaStream_t st = as_stream(stream);
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return MPB_ERR_CUDA;
+  int rc = MPB_OK;
+  for (int g = 0; g < kGroups && rc == MPB_OK; ++g) {
+    if (pl->gcount[g] == 0) continue;
+    float best = 1e30f;
+    Tuning bestt = pl->tune[g];
+    for (const Tuning &c : kCandidates) {
+      pl->tune[g] = c;
+      float ms_sum = 0.0f;
+      for (int rep = 0; rep < 3 && rc == MPB_OK; ++rep) {
+        if (cudaMemsetAsync((uint8_t *)pl->counters + 64 * g, 0, 64, st) != cudaSuccess) rc = MPB_ERR_CUDA;
+        cudaEventRecord(e0, st);
+        const int r = launch_group(pl, g, st, 1.0); /* alone: the whole GPU */
+        cudaEventRecord(e1, st);
+        if (r != MPB_OK || cudaEventSynchronize(e1) != cudaSuccess) rc = MPB_ERR_CUDA;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) ms_sum += ms; /* first run warms up */
+      }
+      if (rc == MPB_OK && ms_sum < best) {
+        best = ms_sum;
+        bestt = c;
+      }
+    }
+    pl->tune[g] = bestt;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+extern "C" int mpb_batch_gemv_get_tuning(const mpb_batch_plan *pl, int prec, int *block, int *blocks_per_sm) {
+  if (!pl || !block || !blocks_per_sm) return MPB_ERR_NULL;
+  const int g = group_of(prec);
+  if (g < 0) return MPB_ERR_PREC;
+  *block = pl->tune[g].block;
+  *blocks_per_sm = pl->tune[g].blocks_per_sm;
+  return MPB_OK;
+}
+
+extern "C" int mpb_batch_gemv_set_tuning(mpb_batch_plan *pl, int prec, int block, int blocks_per_sm) {
+  if (!pl) return MPB_ERR_NULL;
+  const int g = group_of(prec);
+  if (g < 0) return MPB_ERR_PREC;
+  if (block < 32 || block > 256 || block % 32 != 0 || blocks_per_sm < 0 || blocks_per_sm > 64) return MPB_ERR_ARG;
+  pl->tune[g] = Tuning{block, blocks_per_sm};
+  return MPB_OK;
+}
+
+extern "C" void mpb_batch_gemv_destroy(mpb_batch_plan *pl) {
+  if (!pl) return;
+  for (int g = 0; g < kGroups; ++g) {
+    if (pl->aux[g]) cudaStreamDestroy(pl->aux[g]);
+    if (pl->join[g]) cudaEventDestroy(pl->join[g]);
+  }
+  if (pl->fork) cudaEventDestroy(pl->fork);
+  delete pl;
+}

@@ -93,3 +93,29 @@ def test_exact_gemm_complex_workspace(mpb):
     planes = 3 * S * 2 * m * m + 3 * (2 * S - 1) * m * m * 4
     assert planes <= need <= planes + 64 * 1024
     assert L.mpb_gemm_exact_c(256, 8, 8, 8, 4096, 32, 4096, 32, 4096, 32, 16, None, 0, None, None) == -8
+
+
+def test_batch_gemv_plan_validation(mpb):
+    import ctypes as C
+
+    L = mpb.lib()
+    assert L.mpb_batch_gemv_workspace(4096) >= 4096 * 48
+    assert L.mpb_batch_gemv_workspace(0) == 0
+    good = 4096
+    ws = 1 << 20  # fake, 256-aligned; validation fails before it is used
+
+    def one(**kw):
+        d = dict(prec=256, m=4, n=5, lda=32, A=good, x=good, y=good, y_out=good)
+        d.update(kw)
+        arr = (mpb.GemvProblem * 1)(mpb.GemvProblem(**d))
+        h = C.c_void_p()
+        return L.mpb_batch_gemv_plan(1, C.cast(arr, C.c_void_p), ws, 1 << 20, C.byref(h))
+
+    assert one(prec=96) == -1
+    assert one(lda=40) == -5
+    assert one(lda=0) == -5
+    assert one(x=None) == -3
+    assert one(y_out=good + 8) == -4
+    assert one(m=-1) == -2
+    h = C.c_void_p()
+    assert L.mpb_batch_gemv_plan(1, None, ws, 1 << 20, C.byref(h)) == -3
