@@ -2,7 +2,7 @@
 """bench.py -- throughput of the mpb engine on its benchmark workloads.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpb|reference]
-                    [--workload gemm_r512|gemm_c256|axpy_c1024|axpy_r256]
+                    [--workload gemm_r512|gemm_c256|gemv_batch|axpy_c1024|axpy_r256]
 
 One JSON line on stdout (rank 0).  A step is one pass of the hot path over
 one batch of synthetic operands already resident in HBM; K steps are timed
@@ -410,7 +410,150 @@ class GemmWorkload:
                 "l2": "operands > L2 (143 MB real / 71 MB complex); digit and diagonal planes stream through HBM"}
 
 
+class GemvBatchWorkload:
+    """4096 independent GEMV problems y_out = A.x + y of uneven sizes and mixed
+    precisions, planned once, autotuned, and run as one captured CUDA graph
+    (one persistent kernel per precision, largest first) per step.  Operands
+    live in one pool per precision and operand (7.9 GB of tiles > L2)."""
+
+    def __init__(self, name, count, seed):
+        self.name, self.count, self.seed = name, count, seed
+        self.desc = (f"batched GEMV y=A.x+y, {count} independent problems, m,n log-uniform in [16,512], "
+                     "PB uniform in {64,128,256,512,1024,2048}, exponents in [-24,24]; one CUDA graph "
+                     "(persistent kernel per PB, autotuned launch shape) per step")
+
+    default_steps = 20
+
+    def make_host(self, rank):
+        from mpc_cuda_b200 import layout, synth
+
+        probs, pools = synth.gemv_batch(seed=self.seed + 1000 * rank, count=self.count)
+        aos = {p: tuple(layout.aos_from_parts(p, *P[k]) for k in ("A", "x", "y")) for p, P in pools.items()}
+        return probs, aos
+
+    def setup(self, rank, device):
+        import torch
+
+        import mpc_cuda_b200 as M
+        from mpc_cuda_b200 import layout
+
+        self.M = M
+        self.probs, self.aos = self.make_host(rank)
+        self.host = (self.probs, self.aos)
+        self.dev, self.pin, self.stage = {}, {}, {}
+        for p, (A, x, y) in self.aos.items():
+            d = {k: dev_from(layout.aos_to_vec(p, a), device) for k, a in zip(("A", "x", "y"), (A, x, y))}
+            d["yo"] = torch.zeros_like(d["y"])
+            self.dev[p] = d
+            self.pin[p] = {"A": pinned_from(A), "x": pinned_from(x), "y": pinned_from(y),
+                           "yo": torch.empty(y.size, dtype=torch.uint8).pin_memory()}
+            self.stage[p] = {k: torch.empty(v.numel(), dtype=torch.uint8, device=device)
+                             for k, v in self.pin[p].items()}
+        tup = []
+        for pr in self.probs:
+            d, p = self.dev[pr["prec"]], pr["prec"]
+            tup.append((p, pr["m"], pr["n"], pr["lda"], d["A"].data_ptr() + layout.vec_bytes(p, pr["a_off"]),
+                        d["x"].data_ptr() + layout.vec_bytes(p, pr["x_off"]),
+                        d["y"].data_ptr() + layout.vec_bytes(p, pr["y_off"]),
+                        d["yo"].data_ptr() + layout.vec_bytes(p, pr["y_off"])))
+        self.batch = M.BatchGemv(tup)
+        self.batch.autotune()
+        side = torch.cuda.Stream(device)
+        self.batch.run(stream=side.cuda_stream)
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, stream=side):
+            self.batch.run(stream=side.cuda_stream)
+        torch.cuda.synchronize()
+
+    def units(self):
+        return sum(p["m"] * p["n"] for p in self.probs)
+
+    def step(self, i, stream):
+        self.graph.replay()
+
+    @property
+    def launches_per_step(self):
+        return len(self.aos)  # one persistent kernel per precision present
+
+    @property
+    def e2e_launches_per_step(self):
+        return 5 * len(self.aos)  # + pack A, x, y and unpack y_out per precision
+
+    def e2e_step(self, i, stream):
+        M = self.M
+        for p, d in self.dev.items():
+            for k in ("A", "x", "y"):
+                self.stage[p][k].copy_(self.pin[p][k], non_blocking=True)
+                M.pack_aos(p, self.aos[p][("A", "x", "y").index(k)].shape[0], self.stage[p][k], d[k], stream=stream)
+        self.graph.replay()
+        for p, d in self.dev.items():
+            M.unpack_aos(p, self.aos[p][2].shape[0], d["yo"], self.stage[p]["yo"], stream=stream)
+            self.pin[p]["yo"].copy_(self.stage[p]["yo"], non_blocking=True)
+
+    def e2e_bytes(self):
+        h2d = sum(a.size for trip in self.aos.values() for a in trip)
+        return h2d, sum(trip[2].size for trip in self.aos.values())
+
+    def work(self):
+        """per precision: (mp-FMAs, IMAD ops, algorithmic bytes)"""
+        out = {}
+        for pr in self.probs:
+            p, m, n = pr["prec"], pr["m"], pr["n"]
+            N, eb = p // 32, 4 * (p // 32 + 1)
+            u, o, b = out.get(p, (0, 0, 0))
+            out[p] = (u + m * n, o + 2 * N * N * m * n, b + (m * n + n + 2 * m) * eb)
+        return out
+
+    def roofline(self, kernel_s, peaks, imad_ops_s):
+        w = self.work()
+        ops = sum(v[1] for v in w.values())
+        nbytes = sum(v[2] for v in w.values())
+        hbm_peak, hbm_src = peaks
+        imad = ops / kernel_s
+        gbs = nbytes / kernel_s / 1e9
+        tuned = self.batch.tuned_ms()
+        return {"bound": "imad", "achieved": round(imad / 1e9, 1),
+                "peak": round(imad_ops_s / 1e9, 1) if imad_ops_s else None, "unit": "Gop/s",
+                "frac": round(imad / imad_ops_s, 4) if imad_ops_s else None, "ops_per_step": ops,
+                "kernel": "k_batch_gemv<N>, one persistent kernel per PB back to back (one graph replay)",
+                "peak_source": "libmpb_probe.so mad.lo/mad.hi throughput, measured in this run",
+                "traffic": None,
+                "hbm": {"achieved": round(gbs, 1), "peak": hbm_peak["hbm_gbs"], "unit": "GB/s",
+                        "frac": round(gbs / hbm_peak["hbm_gbs"], 4), "bytes_per_step": nbytes,
+                        "peak_source": hbm_src},
+                "per_prec": {str(p): {"mp_fma": v[0], "imad_ops": v[1], "bytes": v[2],
+                                      "solo_ms": round(tuned.get(p, -1.0), 4),
+                                      "tuning": list(self.batch.tuning()[p])} for p, v in sorted(w.items())}}
+
+    def cpu_run(self, impl, count):
+        """Problems in planned order until about count units; returns units done."""
+        import oracle as O
+
+        probs, aos = self.host
+        done = 0
+        for pr in probs:
+            if done >= count:
+                break
+            A, x, y = aos[pr["prec"]]
+            p, m, n = pr["prec"], pr["m"], pr["n"]
+            O.gemv(p, m, n, A[pr["a_off"]:pr["a_off"] + m * pr["lda"]], pr["lda"],
+                   x[pr["x_off"]:pr["x_off"] + n], y[pr["y_off"]:pr["y_off"] + m], impl=impl)
+            done += m * n
+        return done
+
+    cpu_probe_units = 200000
+
+    def config(self):
+        w = self.work()
+        return {"workload": self.desc, "problems": self.count, "mp_fma_per_step": self.units(),
+                "mp_fma_by_prec": {str(p): v[0] for p, v in sorted(w.items())},
+                "units": "mp-FMA (one multiply + one add, each rounded)",
+                "l2": "operand pools 7.9 GB of tiles > L2"}
+
+
 WORKLOADS = {
+    "gemv_batch": lambda: GemvBatchWorkload("gemv_batch", 4096, 0x5EED4),
     "axpy_c1024": lambda: AxpyWorkload("axpy_c1024", True, 1024, 1 << 18, 0x5EED2),
     "axpy_r256": lambda: AxpyWorkload("axpy_r256", False, 256, 1 << 20, 0x5EED1),
     "gemm_r512": lambda: GemmWorkload("gemm_r512", 512, 1024, 1024, 1024, 32,

@@ -133,7 +133,7 @@ size_t mpb_batch_gemv_workspace(int count);
 int mpb_batch_gemv_plan(int count, const mpb_gemv_problem *problems, void *workspace, size_t ws_bytes,
                         mpb_batch_plan **plan);
 /* Run every planned problem: one persistent kernel per precision present,
- * forked onto the plan's streams and joined back into `stream`; no
+ * largest precision first, each over the whole GPU, all on `stream`; no
  * allocation, no host synchronisation (can be captured into a CUDA graph).
  * Runs of one plan must not overlap (they share the workspace queues). */
 int mpb_batch_gemv_run(mpb_batch_plan *plan, void *stream);
@@ -144,6 +144,10 @@ int mpb_batch_gemv_autotune(mpb_batch_plan *plan, void *stream);
  * multiple of 32 up to 256; persistent blocks per SM, 0 = occupancy limit). */
 int mpb_batch_gemv_get_tuning(const mpb_batch_plan *plan, int prec, int *block, int *blocks_per_sm);
 int mpb_batch_gemv_set_tuning(mpb_batch_plan *plan, int prec, int block, int blocks_per_sm);
+/* Time of one run of the precision's problems alone on the whole GPU, as
+ * measured by the last mpb_batch_gemv_autotune (-1 before any; 0 when the
+ * batch has no problem of that precision). */
+int mpb_batch_gemv_tuned_ms(const mpb_batch_plan *plan, int prec, float *ms);
 void mpb_batch_gemv_destroy(mpb_batch_plan *plan);
 
 /* ---- exact-accumulation GEMM on the INT8 tensor cores (no counterpart in the reference) ---- */

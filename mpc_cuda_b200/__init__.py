@@ -70,6 +70,7 @@ _SIGS = {
     "mpb_batch_gemv_autotune": ([_V, _V], C.c_int),
     "mpb_batch_gemv_get_tuning": ([_V, _I, C.POINTER(_I), C.POINTER(_I)], C.c_int),
     "mpb_batch_gemv_set_tuning": ([_V, _I, _I, _I], C.c_int),
+    "mpb_batch_gemv_tuned_ms": ([_V, _I, C.POINTER(C.c_float)], C.c_int),
     "mpb_batch_gemv_destroy": ([_V], None),
     "mpb_gemm_exact_workspace": ([_I, _S, _S, _S, _I], C.c_size_t),
     "mpb_profile_enable": ([_I], None),
@@ -279,6 +280,15 @@ class BatchGemv:
             b, s = C.c_int(), C.c_int()
             _call("mpb_batch_gemv_get_tuning", self._plan, p, C.byref(b), C.byref(s))
             out[p] = (b.value, s.value)
+        return out
+
+    def tuned_ms(self):
+        """{prec: ms of one solo run of that precision's problems} from the last autotune."""
+        out = {}
+        for p in SUPPORTED:
+            v = C.c_float()
+            _call("mpb_batch_gemv_tuned_ms", self._plan, p, C.byref(v))
+            out[p] = v.value
         return out
 
     def set_tuning(self, table):

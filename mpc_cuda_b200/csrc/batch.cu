@@ -7,17 +7,20 @@
  * precision.
  *
  * plan (host, once): validate every descriptor, group the problems by
- * precision, order each group by decreasing cost (n * N^2 per row), split
- * them into 32-row units (one warp each) and upload the descriptors, the
- * problem order and each group's unit prefix sums into the caller's
- * workspace.  run (device, any number of times): reset the queue counters,
- * fork one persistent kernel per precision present onto auxiliary streams,
- * join them back.  Warps claim units from the group's atomic queue, longest
- * problems first, so the uneven batch balances itself.  run allocates
- * nothing and never synchronises the host, so the whole call can be
- * captured into a CUDA graph by the caller.  autotune times each group with
- * every candidate (block size, blocks per SM) on the planned batch and keeps
- * the fastest; set_tuning installs a cached choice.
+ * precision, order each group by decreasing cost (n per row), split them
+ * into 32-row units (one warp each) and upload the descriptors, the problem
+ * order and each group's unit prefix sums into the caller's workspace.
+ * run (device, any number of times): reset the queue counters and launch one
+ * persistent kernel per precision present, largest precision first, each on
+ * the whole GPU.  Warps claim units from the group's atomic queue, longest
+ * problems first, so the uneven batch balances itself.  The groups run one
+ * after the other rather than side by side: a PB=2048 block needs a whole
+ * SM's register file, so concurrent groups fragment the SMs and the largest
+ * group ends up on a fraction of the GPU (measured 2x slower than serial).
+ * run allocates nothing and never synchronises the host, so the caller can
+ * capture it into a CUDA graph.  autotune times each group with every
+ * candidate (block size, blocks per SM) on the planned batch and keeps the
+ * fastest; set_tuning installs a cached choice.
  */
 #include <algorithm>
 #include <mutex>
@@ -124,10 +127,8 @@ struct mpb_batch_plan {
   int *counters;    /* device: one queue counter per group */
   int gstart[kGroups], gcount[kGroups];
   long long gunits[kGroups];
-  double gwork[kGroups]; /* relative cost of each group */
   Tuning tune[kGroups];
-  cudaStream_t aux[kGroups];
-  cudaEvent_t fork, join[kGroups];
+  float tuned_ms[kGroups]; /* autotune: best solo time of the group, -1 before */
 };
 
 static size_t up256b(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -204,8 +205,8 @@ extern "C" int mpb_batch_gemv_plan(int count, const mpb_gemv_problem *problems, 
     pl->gstart[g] = 0;
     pl->gcount[g] = 0;
     pl->gunits[g] = 0;
-    pl->gwork[g] = 0.0;
     pl->tune[g] = Tuning{128, 0}; /* 0: full occupancy */
+    pl->tuned_ms[g] = -1.0f;
   }
   for (int i = 0; i < count; ++i) {
     const mpb_gemv_problem &p = problems[i];
@@ -222,8 +223,6 @@ extern "C" int mpb_batch_gemv_plan(int count, const mpb_gemv_problem *problems, 
       const mpb_gemv_problem &p = problems[idx[pos]];
       pre[pos] = units;
       units += (p.m + 31) / 32;
-      const double N = p.prec / 32.0;
-      pl->gwork[g] += (double)p.m * p.n * N * N;
       ++pos;
     }
     pl->gcount[g] = pos - pl->gstart[g];
@@ -232,11 +231,6 @@ extern "C" int mpb_batch_gemv_plan(int count, const mpb_gemv_problem *problems, 
   bool ok = cudaMemcpy(pl->probs, hp.data(), sizeof(DevProb) * count, cudaMemcpyHostToDevice) == cudaSuccess &&
             cudaMemcpy(pl->order, idx.data(), sizeof(int) * count, cudaMemcpyHostToDevice) == cudaSuccess &&
             cudaMemcpy(pl->prefix, pre.data(), sizeof(long long) * count, cudaMemcpyHostToDevice) == cudaSuccess;
-  for (int g = 0; g < kGroups && ok; ++g) {
-    ok = cudaStreamCreateWithFlags(&pl->aux[g], cudaStreamNonBlocking) == cudaSuccess &&
-         cudaEventCreateWithFlags(&pl->join[g], cudaEventDisableTiming) == cudaSuccess;
-  }
-  ok = ok && cudaEventCreateWithFlags(&pl->fork, cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
     mpb_batch_gemv_destroy(pl);
     return MPB_ERR_CUDA;
@@ -245,7 +239,7 @@ extern "C" int mpb_batch_gemv_plan(int count, const mpb_gemv_problem *problems, 
   return MPB_OK;
 }
 
-static int launch_group(mpb_batch_plan *pl, int g, cudaStream_t st, double share) {
+static int launch_group(mpb_batch_plan *pl, int g, cudaStream_t st) {
   if (pl->gcount[g] == 0 || pl->gunits[g] == 0) return MPB_OK;
   KernelFn fn = kernel_of(g);
   const Tuning t = pl->tune[g];
@@ -253,7 +247,7 @@ static int launch_group(mpb_batch_plan *pl, int g, cudaStream_t st, double share
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, t.block, 0) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   const int bps = t.blocks_per_sm > 0 ? std::min(t.blocks_per_sm, per_sm) : per_sm;
-  long long grid = (long long)std::max(1.0, share * sm_count() * bps + 0.5);
+  long long grid = (long long)sm_count() * bps;
   const long long warps_needed = pl->gunits[g];
   const long long max_grid = (warps_needed * 32 + t.block - 1) / t.block;
   grid = std::min(grid, std::max(1LL, max_grid));
@@ -266,21 +260,11 @@ extern "C" int mpb_batch_gemv_run(mpb_batch_plan *pl, void *stream) {
   if (!pl) return MPB_ERR_NULL;
   cudaStream_t st = as_stream(stream);
   if (cudaMemsetAsync(pl->counters, 0, 64 * kGroups, st) != cudaSuccess) return MPB_ERR_CUDA;
-  double total = 0.0;
-  for (int g = 0; g < kGroups; ++g) total += pl->gwork[g];
-  if (total <= 0.0) return MPB_OK;
-  if (cudaEventRecord(pl->fork, st) != cudaSuccess) return MPB_ERR_CUDA;
-  int rc = MPB_OK;
-  for (int g = 0; g < kGroups; ++g) {
-    if (pl->gcount[g] == 0) continue;
-    if (cudaStreamWaitEvent(pl->aux[g], pl->fork, 0) != cudaSuccess) return MPB_ERR_CUDA;
-    /* each group gets the share of the GPU its work needs, so all finish together */
-    const int r = launch_group(pl, g, pl->aux[g], pl->gwork[g] / total);
-    if (r != MPB_OK) rc = r;
-    if (cudaEventRecord(pl->join[g], pl->aux[g]) != cudaSuccess || cudaStreamWaitEvent(st, pl->join[g], 0) != cudaSuccess)
-      return MPB_ERR_CUDA;
+  for (int g = kGroups - 1; g >= 0; --g) {
+    const int rc = launch_group(pl, g, st);
+    if (rc != MPB_OK) return rc;
   }
-  return rc;
+  return MPB_OK;
 }
 
 extern "C" int mpb_batch_gemv_autotune(mpb_batch_plan *pl, void *stream) {
@@ -299,7 +283,7 @@ extern "C" int mpb_batch_gemv_autotune(mpb_batch_plan *pl, void *stream) {
       for (int rep = 0; rep < 3 && rc == MPB_OK; ++rep) {
         if (cudaMemsetAsync((uint8_t *)pl->counters + 64 * g, 0, 64, st) != cudaSuccess) rc = MPB_ERR_CUDA;
         cudaEventRecord(e0, st);
-        const int r = launch_group(pl, g, st, 1.0); /* alone: the whole GPU */
+        const int r = launch_group(pl, g, st);
         cudaEventRecord(e1, st);
         if (r != MPB_OK || cudaEventSynchronize(e1) != cudaSuccess) rc = MPB_ERR_CUDA;
         float ms = 0.0f;
@@ -312,6 +296,7 @@ extern "C" int mpb_batch_gemv_autotune(mpb_batch_plan *pl, void *stream) {
       }
     }
     pl->tune[g] = bestt;
+    pl->tuned_ms[g] = best / 2.0f;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -327,6 +312,14 @@ extern "C" int mpb_batch_gemv_get_tuning(const mpb_batch_plan *pl, int prec, int
   return MPB_OK;
 }
 
+extern "C" int mpb_batch_gemv_tuned_ms(const mpb_batch_plan *pl, int prec, float *ms) {
+  if (!pl || !ms) return MPB_ERR_NULL;
+  const int g = group_of(prec);
+  if (g < 0) return MPB_ERR_PREC;
+  *ms = pl->gcount[g] > 0 ? pl->tuned_ms[g] : 0.0f;
+  return MPB_OK;
+}
+
 extern "C" int mpb_batch_gemv_set_tuning(mpb_batch_plan *pl, int prec, int block, int blocks_per_sm) {
   if (!pl) return MPB_ERR_NULL;
   const int g = group_of(prec);
@@ -338,10 +331,5 @@ extern "C" int mpb_batch_gemv_set_tuning(mpb_batch_plan *pl, int prec, int block
 
 extern "C" void mpb_batch_gemv_destroy(mpb_batch_plan *pl) {
   if (!pl) return;
-  for (int g = 0; g < kGroups; ++g) {
-    if (pl->aux[g]) cudaStreamDestroy(pl->aux[g]);
-    if (pl->join[g]) cudaEventDestroy(pl->join[g]);
-  }
-  if (pl->fork) cudaEventDestroy(pl->fork);
   delete pl;
 }

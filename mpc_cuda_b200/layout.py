@@ -68,7 +68,7 @@ def _tiles_from(prec: int, limbs: np.ndarray, heads: np.ndarray) -> np.ndarray:
     L[:n] = limbs
     H = np.full(T * 32, HEAD_ZERO, dtype=np.uint32)
     H[:n] = heads
-    L = L.reshape(T, 32, G, V).transpose(0, 2, 1, 3).reshape(T, -1)
+    L = L.reshape(T, 32, G, V).transpose(0, 2, 1, 3).reshape(T, 32 * N)
     return np.concatenate([L, H.reshape(T, 32)], axis=1)  # (T, tile words)
 
 

@@ -103,6 +103,58 @@ def gemv_batch_shapes(seed: int = 0x5EED4, count: int = 4096):
     return np.clip(m, 16, 512), np.clip(n, 16, 512), prec
 
 
+def _round32(v):
+    return -(-np.asarray(v, dtype=np.int64) // 32) * 32
+
+
+def gemv_batch(seed: int = 0x5EED4, count: int = 4096, shapes=None, exp_lo: int = -24, exp_hi: int = 24):
+    """The batched GEMV workload, generated one precision group at a time.
+
+    Returns ``(problems, pools)``.  ``problems[i]`` is a dict with ``prec, m,
+    n, lda`` (``lda`` = n rounded up to 32) and element offsets ``a_off,
+    x_off, y_off`` into its precision's pools; every offset is a multiple of
+    32, so each operand starts on a tile boundary of the device layout.
+    ``pools[prec]`` holds ``A``, ``x``, ``y`` as ``(limbs, heads)`` with the
+    padding columns of A and the tails of x and y set to exact zeros.
+    """
+    m, n, prec = shapes if shapes is not None else gemv_batch_shapes(seed, count)
+    m, n, prec = np.asarray(m), np.asarray(n), np.asarray(prec)
+    rng = np.random.default_rng(seed ^ 0xB47C)
+    problems = [None] * len(m)
+    pools = {}
+    for p in sorted(set(int(v) for v in prec)):
+        idx = np.nonzero(prec == p)[0]
+        lda = np.maximum(32, _round32(n[idx]))
+        a_sz, x_sz, y_sz = m[idx] * lda, _round32(n[idx]), _round32(m[idx])
+        a_off = np.concatenate([[0], np.cumsum(a_sz)[:-1]])
+        x_off = np.concatenate([[0], np.cumsum(x_sz)[:-1]])
+        y_off = np.concatenate([[0], np.cumsum(y_sz)[:-1]])
+        A = random_elems(rng, p, int(a_sz.sum()), exp_lo, exp_hi)
+        x = random_elems(rng, p, int(x_sz.sum()), exp_lo, exp_hi)
+        y = random_elems(rng, p, int(y_sz.sum()), exp_lo, exp_hi)
+        a_pad = np.concatenate([np.tile(np.arange(ld) >= c, r) for r, c, ld in zip(m[idx], n[idx], lda)])
+        x_pad = np.concatenate([np.arange(s) >= c for c, s in zip(n[idx], x_sz)])
+        y_pad = np.concatenate([np.arange(s) >= r for r, s in zip(m[idx], y_sz)])
+        for (limbs, heads), pad in ((A, a_pad), (x, x_pad), (y, y_pad)):
+            limbs[pad] = 0
+            heads[pad] = HEAD_ZERO
+        pools[p] = dict(A=A, x=x, y=y)
+        for j, i in enumerate(idx):
+            problems[i] = dict(prec=p, m=int(m[i]), n=int(n[i]), lda=int(lda[j]), a_off=int(a_off[j]),
+                               x_off=int(x_off[j]), y_off=int(y_off[j]))
+    return problems, pools
+
+
+def gemv_batch_problem(pools, pr):
+    """One problem's operands ``(A, x, y)`` as (limbs, heads), A dense m x n."""
+    P, m, n, lda = pools[pr["prec"]], pr["m"], pr["n"], pr["lda"]
+    la, ha = P["A"]
+    sel = slice(pr["a_off"], pr["a_off"] + m * lda)
+    A = (la[sel].reshape(m, lda, -1)[:, :n].reshape(m * n, -1), ha[sel].reshape(m, lda)[:, :n].reshape(-1))
+    xs, ys = slice(pr["x_off"], pr["x_off"] + n), slice(pr["y_off"], pr["y_off"] + m)
+    return A, (P["x"][0][xs], P["x"][1][xs]), (P["y"][0][ys], P["y"][1][ys])
+
+
 def interleave_complex(prec: int, re, im):
     """(re parts, im parts) -> complex AoS bytes of cu_fcomplex<prec>."""
     from .layout import aos_from_parts

@@ -28,7 +28,7 @@ def make_batch(count, seed, lo=1, hi=130, exps=24, precs=layout.SUPPORTED, empti
         y = synth.random_elems(rng, prec, mi, -exps, exps)
         L = np.zeros((mi, lda, prec // 32), np.uint32)
         H = np.full((mi, lda), layout.HEAD_ZERO, np.uint32)
-        L[:, :ni] = A[0].reshape(mi, ni, -1)
+        L[:, :ni] = A[0].reshape(mi, ni, prec // 32)
         H[:, :ni] = A[1].reshape(mi, ni)
         probs.append(dict(prec=prec, m=mi, n=ni, lda=lda, A=(A[0], A[1]), x=x, y=y,
                           dA=to_dev(layout.vec_from_parts(prec, L.reshape(mi * lda, -1), H.reshape(-1)))
@@ -99,19 +99,53 @@ def test_batch_graph_capture_autotune_and_replay(orc, mpb):
     b.close()
 
 
+def upload_batch(probs, pools):
+    """Device pools (one tiled buffer per precision and operand) and the
+    BatchGemv problem tuples pointing into them."""
+    import torch
+
+    dev = {}
+    for prec, P in pools.items():
+        dev[prec] = {k: to_dev(layout.vec_from_parts(prec, *P[k])) for k in ("A", "x", "y")}
+        dev[prec]["yo"] = torch.zeros_like(dev[prec]["y"])
+    tup = []
+    for pr in probs:
+        d, vb = dev[pr["prec"]], (lambda off, p=pr["prec"]: layout.vec_bytes(p, off))
+        tup.append((pr["prec"], pr["m"], pr["n"], pr["lda"], d["A"].data_ptr() + vb(pr["a_off"]),
+                    d["x"].data_ptr() + vb(pr["x_off"]), d["y"].data_ptr() + vb(pr["y_off"]),
+                    d["yo"].data_ptr() + vb(pr["y_off"])))
+    return dev, tup
+
+
 def test_batch_full_size_4096_problems(orc, mpb):
     """The batched workload at full size: 4096 problems, m, n log-uniform in
     [16, 512], PB uniform over the six precisions, exponents in [-24, 24].
     Every result equals the single-problem kernel's; a sample equals MPFR."""
-    probs = make_batch(4096, 0x5EED4, lo=16, hi=512, empties=False)
-    b = plan(mpb, probs)
+    import torch
+
+    probs, pools = synth.gemv_batch()
+    dev, tup = upload_batch(probs, pools)
+    b = mpb.BatchGemv(tup)
+    b.autotune()
+    for d in dev.values():
+        d["yo"].zero_()
     b.run()
-    batched = [got(p) for p in probs]
-    for i, p in enumerate(probs):
-        mpb.gemv(p["prec"], p["m"], p["n"], p["dA"], p["lda"], p["dx"], p["dy"], p["dyo"])
-        assert np.array_equal(batched[i], got(p)), f"problem {i} differs from mpb_gemv_r"
+    torch.cuda.synchronize()
+    batched = {p: to_host(d["yo"]) for p, d in dev.items()}
+    for d in dev.values():
+        d["yo"].zero_()
+    for t in tup:
+        mpb.gemv(t[0], t[1], t[2], t[4], t[3], t[5], t[6], t[7])
+    torch.cuda.synchronize()
+    for p, d in dev.items():
+        assert np.array_equal(batched[p], to_host(d["yo"])), f"PB={p}: batched results differ from mpb_gemv_r"
     rng = np.random.default_rng(3)
     for i in rng.choice(len(probs), 24, replace=False):
-        p = probs[i]
-        assert orc.mismatches(p["prec"], batched[i], expected(orc, p))[0] == 0, i
+        pr = probs[i]
+        prec, m, n = pr["prec"], pr["m"], pr["n"]
+        A, x, y = synth.gemv_batch_problem(pools, pr)
+        want = orc.gemv(prec, m, n, layout.aos_from_parts(prec, *A), n, layout.aos_from_parts(prec, *x),
+                        layout.aos_from_parts(prec, *y), impl="mp")
+        tiles = batched[prec][layout.vec_bytes(prec, pr["y_off"]):]
+        assert orc.mismatches(prec, layout.vec_to_aos(prec, tiles, m), want)[0] == 0, i
     b.close()

@@ -62,3 +62,34 @@ def test_generators_shape_and_distribution():
     assert 0.003 < (~nz).mean() < 0.02
     m, n, p = synth.gemv_batch_shapes(count=4096)
     assert m.min() >= 16 and m.max() <= 512 and set(np.unique(p)) <= set(layout.SUPPORTED)
+
+
+def test_gemv_batch_pools_are_tile_aligned_and_zero_padded(orc):
+    """The batched GEMV workload generator: every operand starts on a tile
+    boundary, padding is exact zeros, and a problem's operands come back out
+    of the pools with the shapes the problem names."""
+    m, n, prec = synth.gemv_batch_shapes(count=60)
+    assert m.min() >= 16 and m.max() <= 512 and n.min() >= 16 and n.max() <= 512
+    assert set(prec.tolist()) <= set(layout.SUPPORTED)
+    probs, pools = synth.gemv_batch(count=60)
+    assert len(probs) == 60
+    for pr in probs:
+        assert pr["lda"] % 32 == 0 and pr["lda"] >= pr["n"]
+        assert pr["a_off"] % 32 == 0 and pr["x_off"] % 32 == 0 and pr["y_off"] % 32 == 0
+        P = pools[pr["prec"]]
+        la, ha = P["A"]
+        rows = ha[pr["a_off"]:pr["a_off"] + pr["m"] * pr["lda"]].reshape(pr["m"], pr["lda"])
+        assert (rows[:, pr["n"]:] == layout.HEAD_ZERO).all() and (rows[:, :pr["n"]] != layout.HEAD_ZERO).all()
+        A, x, y = synth.gemv_batch_problem(pools, pr)
+        N = pr["prec"] // 32
+        assert A[0].shape == (pr["m"] * pr["n"], N) and x[0].shape == (pr["n"], N) and y[0].shape == (pr["m"], N)
+        assert (A[0][:, -1] >> 31).all() and (x[0][:, -1] >> 31).all()
+    # a sample through the oracle: the AoS of the padded pool with lda gives the dense problem's result
+    pr = min(probs, key=lambda p: p["m"] * p["n"])
+    p = pr["prec"]
+    A, x, y = synth.gemv_batch_problem(pools, pr)
+    dense = orc.gemv(p, pr["m"], pr["n"], layout.aos_from_parts(p, *A), pr["n"], layout.aos_from_parts(p, *x),
+                     layout.aos_from_parts(p, *y))
+    Ap = layout.aos_from_parts(p, *pools[p]["A"])[pr["a_off"]:pr["a_off"] + pr["m"] * pr["lda"]]
+    padded = orc.gemv(p, pr["m"], pr["n"], Ap, pr["lda"], layout.aos_from_parts(p, *x), layout.aos_from_parts(p, *y))
+    assert orc.mismatches(p, dense, padded)[0] == 0
