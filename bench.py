@@ -326,6 +326,8 @@ class GemmWorkload:
         self.dC2 = M.empty(self.prec, self.m * self.n, c, device=device)
         self.ws = torch.empty(M.gemm_exact_workspace(self.prec, self.m, self.n, self.k, self.sp_bits, c),
                               dtype=torch.uint8, device=device)
+        S, self.d0, self.pairs = M.gemm_exact_info(self.prec, self.m, self.n, self.k, self.sp_bits, c)
+        assert S == self.S, (S, self.S)
         self.status = torch.zeros(2, dtype=torch.int32, device=device)
         self.hA, self.hB = pinned_from(A), pinned_from(B)
         self.hC = torch.empty(self.m * self.n * A.shape[1], dtype=torch.uint8).pin_memory()
@@ -378,12 +380,12 @@ class GemmWorkload:
         return {"plain_ms_per_step": plain_ms, "plain_value": self.units() / (plain_ms / 1e3), "status": st}
 
     def roofline_tensor(self, tensor_ms, int8_ops):
-        ops = 2.0 * self.nprod * self.units() * self.S * self.S
+        ops = 2.0 * self.nprod * self.units() * self.pairs
         achieved = ops / (tensor_ms / 1e3)
         return {"bound": "tensor", "achieved": round(achieved / 1e12, 1), "unit": "TOP/s (int8)",
                 "peak": round(int8_ops / 1e12, 1) if int8_ops else None,
                 "frac": round(achieved / int8_ops, 4) if int8_ops else None,
-                "ops_per_unit": 2 * self.nprod * self.S * self.S, "kernel": "k_diag_gemm (tcgen05.mma kind::i8)",
+                "ops_per_unit": 2 * self.nprod * self.pairs, "kernel": "k_diag_gemm (tcgen05.mma kind::i8)",
                 "kernel_ms": round(tensor_ms, 4),
                 "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm), measured in this run",
                 "traffic": None}
@@ -404,7 +406,8 @@ class GemmWorkload:
 
     def config(self):
         return {"workload": self.desc, "prec": self.prec, "m": self.m, "n": self.n, "k": self.k,
-                "sp_bits": self.sp_bits, "slices": self.S,
+                "sp_bits": self.sp_bits, "slices": self.S, "first_diagonal": getattr(self, "d0", None),
+                "slice_pairs": getattr(self, "pairs", None),
                 "units": ("complex mp-FMA (one complex product accumulated)" if self.cplx
                           else "mp-FMA (one exact product accumulated)"),
                 "l2": "operands > L2 (143 MB real / 71 MB complex); digit and diagonal planes stream through HBM"}

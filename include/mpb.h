@@ -54,7 +54,8 @@ int mpb_prec_supported(int prec);              /* 1 if prec is one of the suppor
  * mpb_profile_enable(1) clears previous records and makes multi-kernel entry
  * points (mpb_gemm_exact_r) record a CUDA event pair around each phase on the
  * caller's stream: 0 exponent statistics, 1 slicing, 2 tensor-core GEMM,
- * 3 exact rounding, 4 fallback.  mpb_profile_phase_ms waits for the recorded
+ * 3 exact rounding (first pass), 4 fallback, 5 tensor-core recomputation of
+ * the low diagonals for tiles whose truncated sum did not certify.  mpb_profile_phase_ms waits for the recorded
  * events and returns the phase's total time in ms over every call since
  * enabling (-1 if none); mpb_profile_phase_count returns the number of calls
  * recorded.  Not thread-safe against concurrent enable.  No counterpart in the
@@ -160,8 +161,12 @@ void mpb_batch_gemv_destroy(mpb_batch_plan *plan);
  * aligned, owned by the caller; calls sharing a workspace must not overlap.
  * status: optional device int[2], written asynchronously: [0] = number of rows
  * plus columns that took the fallback, [1] = 0 or an internal kernel error code.
- * The slice budget costs S^2 int8 tensor-core products per multiply-add,
- * S = ceil((prec + sp_bits + 2) / 8); sp_bits <= 118 is supported. */
+ * The slice budget costs S = ceil((prec + sp_bits + 2) / 8) digit slices;
+ * sp_bits <= 118 is supported.  The low-order slice pairs, which only reach
+ * bits far below each result's ULP, are skipped, and each rounding is
+ * certified against a bound on what they could add; an entry that does not
+ * certify (heavy cancellation, or a sum next to a rounding midpoint) is
+ * recomputed from the full sum, so the result is always correctly rounded. */
 size_t mpb_gemm_exact_workspace(int prec, size_t m, size_t n, size_t k, int sp_bits);
 size_t mpb_gemm_exact_c_workspace(int prec, size_t m, size_t n, size_t k, int sp_bits);
 int mpb_gemm_exact_r(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
@@ -173,6 +178,12 @@ int mpb_gemm_exact_r(int prec, size_t m, size_t n, size_t k, const void *A, size
  * mpb_gemm_exact_c_workspace. */
 int mpb_gemm_exact_c(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
                      void *C, size_t ldc, int sp_bits, void *workspace, size_t ws_bytes, int *status, void *stream);
+/* Geometry of an exact GEMM call (cplx 0 real, 1 complex): the number of digit
+ * slices S, the lowest diagonal the tensor cores compute for every tile, and
+ * the slice pairs that costs per real product and multiply-add (the int8
+ * tensor-core work is 2 * pairs * m * n * k per real product). */
+int mpb_gemm_exact_plan_info(int prec, size_t m, size_t n, size_t k, int sp_bits, int cplx, int *slices,
+                             int *first_diag, long long *pairs);
 /* The same exact GEMM for callers that cannot allocate device memory (a
  * latency-critical loop that must not call cudaMalloc after start-up, or a
  * framework that owns the whole memory pool): no workspace argument and no

@@ -64,6 +64,8 @@ _SIGS = {
     "mpb_gemv_c": ([_I, _S, _S, _V, _S, _V, _V, _V, _V], C.c_int),
     "mpb_gemm_r": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _V], C.c_int),
     "mpb_gemm_c": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _V], C.c_int),
+    "mpb_gemm_exact_plan_info": ([_I, _S, _S, _S, _I, _I, C.POINTER(_I), C.POINTER(_I), C.POINTER(C.c_longlong)],
+                                 C.c_int),
     "mpb_batch_gemv_workspace": ([_I], C.c_size_t),
     "mpb_batch_gemv_plan": ([_I, _V, _V, _S, C.POINTER(_V)], C.c_int),
     "mpb_batch_gemv_run": ([_V, _V], C.c_int),
@@ -223,6 +225,14 @@ def gemm_exact_workspace(prec, m, n, k, sp_bits=32, cplx=False):
     return int(f(prec, m, n, k, sp_bits))
 
 
+def gemm_exact_info(prec, m, n, k, sp_bits=32, cplx=False):
+    """(slices S, lowest tensor-core diagonal d0, slice pairs per real product)."""
+    S, d0, pairs = C.c_int(), C.c_int(), C.c_longlong()
+    _call("mpb_gemm_exact_plan_info", prec, m, n, k, sp_bits, 1 if cplx else 0, C.byref(S), C.byref(d0),
+          C.byref(pairs))
+    return S.value, d0.value, pairs.value
+
+
 def gemm_exact(prec, m, n, k, A, lda, B, ldb, Cm, ldc, sp_bits=32, workspace=None, status=None,
                cplx=False, stream=None):
     """C = A.B with one rounding per entry (exact accumulation on the INT8
@@ -310,6 +320,7 @@ class BatchGemv:
 __all__ = [
     "SUPPORTED", "MpbError", "aos_bytes", "tile_bytes", "vec_bytes", "build", "lib", "host_lib", "empty",
     "empty_matrix", "pack_aos", "unpack_aos", "from_double", "to_double", "binop", "fma", "axpy", "gemv", "gemm",
-    "layout", "MPB_OP_MUL", "MPB_OP_ADD", "MPB_OP_SUB", "gemm_exact", "gemm_exact_workspace", "BatchGemv",
+    "layout", "MPB_OP_MUL", "MPB_OP_ADD", "MPB_OP_SUB", "gemm_exact", "gemm_exact_workspace", "gemm_exact_info",
+    "BatchGemv",
     "GemvProblem",
 ]

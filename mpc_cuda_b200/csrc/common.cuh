@@ -38,7 +38,15 @@ int sm_count();
 
 /* Opt-in phase timing (mpb_profile_enable): entry points that run several
  * kernels record a CUDA event pair around each phase on the caller's stream. */
-enum { kPhaseStats = 0, kPhaseSlice = 1, kPhaseTensor = 2, kPhaseRound = 3, kPhaseFallback = 4, kPhases = 5 };
+enum {
+  kPhaseStats = 0,
+  kPhaseSlice = 1,
+  kPhaseTensor = 2,
+  kPhaseRound = 3,
+  kPhaseFallback = 4,
+  kPhaseTensorLow = 5, /* recomputation of the low diagonals of marked tiles */
+  kPhases = 6
+};
 void profile_mark(int phase, bool begin, cudaStream_t st);
 
 /* Grid for a grid-stride kernel over `work` warp-sized units of 32 threads

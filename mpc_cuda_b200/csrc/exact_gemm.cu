@@ -34,13 +34,24 @@
  *    products' sum_d 256^d D_d is streamed word by word into 32-bit limbs with
  *    an int64 carry, normalised and rounded once (RNDN) to PB bits with
  *    exponent E_i + F_j - 2PB - 2SP + msb + 1.
+ * 5. Truncation.  The low diagonals d < d0 only reach the bits far below the
+ *    result's ULP, so the main pass skips them (about 40% of the pairs at
+ *    PB=512): their sum is bounded, |R| < 2^cert, and the rounding of the
+ *    truncated sum is accepted only when no value within 2^cert of it rounds
+ *    differently (round_words).  An entry that fails -- heavy cancellation,
+ *    or a sum within 2^cert of a rounding midpoint -- marks its output tile;
+ *    the tensor cores then compute the low diagonals of the marked tiles only,
+ *    and a second rounding pass rounds those entries from the full, exact
+ *    sum.  Every entry is therefore still the correctly rounded dot product.
  *
  * This file holds the kernels and the entry points; each precision's
  * instantiations are compiled in their own translation unit
  * (exact_gemm_pb*.cu) so the build runs them in parallel.
  *
- * Work: nprod*2*m*n*k*S^2 int8 operations (S = ceil((PB+SP+2)/8) real,
- * ceil((PB+SP+3)/8) complex; S = 69 at PB=512 with a 32-bit budget).
+ * Work: nprod*2*m*n*k*pairs int8 operations, pairs = the slice pairs on the
+ * diagonals [d0, 2S-2] (mpb_gemm_exact_plan_info; S = ceil((PB+SP+2)/8)
+ * real, ceil((PB+SP+3)/8) complex; S = 69, d0 = 63, 2745 of S^2 = 4761
+ * pairs at PB=512, k=1024 with a 32-bit budget).
  * Scratch (caller-provided workspace, mpb_gemm_exact_workspace /
  * mpb_gemm_exact_c_workspace): digit planes nprod*S*(m+n)*kp bytes and the
  * diagonal planes nprod*P*(2S-1)*m*n*4 bytes.
@@ -53,19 +64,25 @@ namespace exact {
 struct Unit {
   int d, q, ti, tj, part, s_lo, s_hi, kc0, kc1;
 };
-/* units ordered by decreasing diagonal length (longest first) */
-__device__ __forceinline__ Unit decode(const GemmArgs &g, long u) {
+/* unit u of a launch over T tiles: units ordered by decreasing diagonal
+ * length (the r-th longest diagonal of [dl, dh], alternating around S-1),
+ * then product, tile, k-part */
+__device__ __forceinline__ Unit decode(const GemmArgs &g, long u, long T) {
   Unit x;
-  const long tiles = (long)g.mt * g.nt;
-  const long per = (long)g.nprod * tiles * g.P;
+  const long per = (long)g.nprod * T * g.P;
   const int r = (int)(u / per);
   long rem = u % per;
-  x.q = (int)(rem / (tiles * g.P));
-  rem %= tiles * g.P;
-  const int tile = (int)(rem / g.P);
+  x.q = (int)(rem / (T * g.P));
+  rem %= T * g.P;
+  const long t = rem / g.P;
   x.part = (int)(rem % g.P);
-  const int h = (r + 1) / 2;
-  x.d = (r == 0) ? g.S - 1 : ((r & 1) ? g.S - 1 - h : g.S - 1 + h);
+  const int tile = g.tiles ? g.tiles[t] : (int)t;
+  const int c = min(max(g.S - 1, g.dl), g.dh);
+  const int a = c - g.dl, b = g.dh - c, mm = min(a, b);
+  if (r <= 2 * mm)
+    x.d = (r == 0) ? c : ((r & 1) ? c - (r + 1) / 2 : c + r / 2);
+  else
+    x.d = (a > b) ? c - (r - mm) : c + (r - mm);
   x.ti = tile / g.nt;
   x.tj = tile % g.nt;
   x.s_lo = max(0, x.d - g.S + 1);
@@ -88,6 +105,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   __shared__ volatile int abort_flag;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  /* tiles in this launch, and its unit count (a tile list is counted by the
+   * previous kernel on the stream) */
+  const long T = g.tiles ? (long)*g.ntiles : (long)g.mt * g.nt;
+  const long units = g.tiles ? T * g.nprod * (g.dh - g.dl + 1) * g.P : g.units;
   if (threadIdx.x == 0) {
     abort_flag = 0;
     for (int s = 0; s < STAGES; ++s) {
@@ -124,8 +145,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
-      for (long u = blockIdx.x; u < g.units && !abort_flag; u += gridDim.x) {
-        const Unit x = decode(g, u);
+      for (long u = blockIdx.x; u < units && !abort_flag; u += gridDim.x) {
+        const Unit x = decode(g, u, T);
         for (int s = x.s_lo; s <= x.s_hi && !abort_flag; ++s) {
           const int t = x.d - s;
           for (int kc = x.kc0; kc < x.kc1; ++kc) {
@@ -160,8 +181,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       uint32_t phase = 0;
       int acc = 0;
       uint32_t aphase = 0;
-      for (long u = blockIdx.x; u < g.units && !abort_flag; u += gridDim.x) {
-        const Unit x = decode(g, u);
+      for (long u = blockIdx.x; u < units && !abort_flag; u += gridDim.x) {
+        const Unit x = decode(g, u, T);
         if (!sm100::mbar_wait(&tempty[acc], aphase ^ 1u, &abort_flag)) {
           fail(2);
           break;
@@ -210,7 +231,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     const int q = warp & 3; /* TMEM lane quarter this warp may access */
     int acc = 0;
     uint32_t aphase = 0;
-    for (long u = blockIdx.x; u < g.units; u += gridDim.x) {
+    for (long u = blockIdx.x; u < units; u += gridDim.x) {
       /* tcgen05.ld is warp-collective: lane 0 waits and decides for the warp */
       int ok = 1;
       if (lane == 0) ok = (!abort_flag && sm100::mbar_wait(&tfull[acc], aphase, &abort_flag)) ? 1 : 0;
@@ -219,7 +240,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         if (lane == 0) fail(4);
         break;
       }
-      const Unit x = decode(g, u);
+      const Unit x = decode(g, u, T);
       sm100::tc_fence_after();
       const int row = x.ti * BM + q * 32 + lane;
       int32_t *drow = g.D + ((((size_t)x.q * g.P + x.part) * (2 * g.S - 1) + x.d) * g.m + (size_t)row) * g.n;
@@ -290,7 +311,8 @@ static bool make_tmap(CUtensorMap *tm, void *base, int kp, int rows, int planes,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *err, cudaStream_t st) {
+int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *err, int dl, int dh,
+                     const int *tiles, const int *ntiles, cudaStream_t st) {
   CUtensorMap tmA, tmB;
   if (!make_tmap(&tmA, Asl, p.kp, p.m, p.nprod * p.S, BM) || !make_tmap(&tmB, Bsl, p.kp, p.n, p.nprod * p.S, BN))
     return MPB_ERR_CUDA;
@@ -306,13 +328,18 @@ int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *e
   ga.KC = p.KC;
   ga.m = p.m;
   ga.n = p.n;
-  ga.units = p.units;
+  ga.dl = dl;
+  ga.dh = dh;
+  ga.units = (long)p.nprod * (dh - dl + 1) * p.mt * p.nt * p.P;
+  ga.tiles = tiles;
+  ga.ntiles = ntiles;
   ga.D = D;
   ga.err = err;
-  const long grid = std::min<long>(p.units, (long)sm_count());
-  profile_mark(kPhaseTensor, true, st);
+  const long grid = std::min<long>(ga.units, (long)sm_count());
+  const int phase = tiles ? kPhaseTensorLow : kPhaseTensor;
+  profile_mark(phase, true, st);
   k_diag_gemm<<<(int)grid, kGemmThreads, kSmemBytes, st>>>(tmA, tmB, ga);
-  profile_mark(kPhaseTensor, false, st);
+  profile_mark(phase, false, st);
   return launch_status();
 }
 
@@ -334,6 +361,20 @@ extern "C" size_t mpb_gemm_exact_workspace(int prec, size_t m, size_t n, size_t 
 }
 extern "C" size_t mpb_gemm_exact_c_workspace(int prec, size_t m, size_t n, size_t k, int sp_bits) {
   return workspace_bytes(prec, m, n, k, sp_bits, 1);
+}
+
+extern "C" int mpb_gemm_exact_plan_info(int prec, size_t m, size_t n, size_t k, int sp_bits, int cplx, int *slices,
+                                        int *first_diag, long long *pairs) {
+  if (!prec_ok(prec)) return MPB_ERR_PREC;
+  if (m == 0 || n == 0 || k == 0 || m > (1u << 24) || n > (1u << 24) || k > (1u << 24)) return MPB_ERR_SIZE;
+  exact::Plan p;
+  if (!exact::make_plan(prec, m, n, k, sp_bits, cplx, p)) return MPB_ERR_ARG;
+  long long pr = 0;
+  for (int d = p.d0; d <= 2 * p.S - 2; ++d) pr += std::min(d, 2 * p.S - 2 - d) + 1;
+  if (slices) *slices = p.S;
+  if (first_diag) *first_diag = p.d0;
+  if (pairs) *pairs = pr;
+  return MPB_OK;
 }
 
 static int exact_entry(int cplx, int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B,

@@ -25,6 +25,12 @@ constexpr uint32_t B_STAGE = BN * BK; /* 32 KB */
 constexpr int kGemmThreads = 192;   /* warp 0 TMA, warp 1 MMA, warps 2-5 epilogue */
 constexpr long kSafeTerms = 1L << 17; /* pairs * k < 2^17 keeps |D| < 2^31 */
 constexpr int kMaxParts = 16;       /* keeps the rounding's int64 word sums exact */
+/* Low-diagonal truncation: the main pass computes diagonals d >= d0 only.
+ * d0 is the lowest diagonal for which an entry whose magnitude is up to
+ * kDeltaBits below the largest possible product (cancellation or small
+ * entries) still certifies its rounding with kMarginBits to spare. */
+constexpr int kDeltaBits = 40;
+constexpr int kMarginBits = 16;
 constexpr size_t kSmemBytes = 1024 /* alignment slack */ + STAGES * (A_STAGE + B_STAGE) + 256 /* barriers */;
 
 /* the per-call geometry (host and device) */
@@ -33,9 +39,17 @@ struct Plan {
   int m, n, k, kp, KC; /* kp = k padded to BK, KC = kp / BK chunks */
   int P, cpp;          /* k-parts per diagonal, chunks per part */
   int mt, nt;          /* tiles */
-  long units;
-  size_t off_rowE, off_colE, off_flags, off_cnt, off_asl, off_bsl, off_d, total;
+  int d0;              /* lowest diagonal of the main pass (0: all diagonals, no certification) */
+  long cert;           /* log2 of the bound on the omitted diagonals' sum (LSB units); -1 when d0 = 0 */
+  long units;          /* units of the main pass, diagonals [d0, 2S-2] */
+  size_t off_rowE, off_colE, off_flags, off_cnt, off_ef, off_tf, off_tiles, off_asl, off_bsl, off_d, total;
 };
+
+static inline int ceil_log2(long x) {
+  int r = 0;
+  while ((1L << r) < x) ++r;
+  return r;
+}
 
 static inline size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -65,7 +79,27 @@ static bool make_plan(int prec, size_t m, size_t n, size_t k, int sp_bits, int c
   if (p.P > kMaxParts) return false;
   p.mt = (int)((m + BM - 1) / BM);
   p.nt = (int)((n + BN - 1) / BN);
-  p.units = (long)p.nprod * (2 * p.S - 1) * p.mt * p.nt * p.P;
+  /* The omitted sum R = sum_{d<d0} 256^d D_d has |D_d| <= c*kp*(d+1)*2^14
+   * (c = sum of the |coefficients| of the products in one component: 1 real,
+   * at most 3 complex), so |R| < c*kp*d0*2^(6.006)*256^d0 <= 2^cert with
+   * cert = 8*d0 + 7 + ceil(log2(c*kp*d0)).  The largest possible product has
+   * its top bit at 2*PB + 2*SP - 1; a result kDeltaBits below that has its
+   * ULP at PB + 2*SP - kDeltaBits, and cert must stay kMarginBits under it. */
+  {
+    const int c = cplx ? 3 : 1;
+    const long budget = (long)prec + 2L * p.SP - kDeltaBits - kMarginBits;
+    p.d0 = 0;
+    p.cert = -1;
+    for (int d = p.S - 1; d >= 1; --d) {
+      const long cert = 8L * d + 7 + ceil_log2((long)c * p.kp * d);
+      if (cert <= budget) {
+        p.d0 = d;
+        p.cert = cert;
+        break;
+      }
+    }
+  }
+  p.units = (long)p.nprod * (2 * p.S - 1 - p.d0) * p.mt * p.nt * p.P;
   size_t o = 0;
   p.off_rowE = o;
   o = up256(o + 4 * m);
@@ -73,8 +107,14 @@ static bool make_plan(int prec, size_t m, size_t n, size_t k, int sp_bits, int c
   o = up256(o + 4 * n);
   p.off_flags = o; /* m row flags then n column flags, one byte each */
   o = up256(o + m + n);
-  p.off_cnt = o;
+  p.off_cnt = o; /* [0] fallback rows+cols, [1] kernel error, [2] tiles to recompute */
   o = up256(o + 16);
+  p.off_ef = o; /* one byte per entry: 1 = rounding not certified, recomputed */
+  o = up256(o + m * n);
+  p.off_tf = o; /* one int per output tile: marked for recomputation */
+  o = up256(o + 4 * (size_t)p.mt * p.nt);
+  p.off_tiles = o; /* list of marked tiles */
+  o = up256(o + 4 * (size_t)p.mt * p.nt);
   p.off_asl = o;
   o = up256(o + (size_t)p.nprod * p.S * m * p.kp);
   p.off_bsl = o;
@@ -324,14 +364,20 @@ __global__ void __launch_bounds__(256) k_slice_b(int n, int k, int kp, const uin
  * ------------------------------------------------------------------ */
 struct GemmArgs {
   int S, nprod, mt, nt, P, cpp, KC, m, n;
-  long units;
-  int32_t *D; /* [nprod][P][2S-1][m][n] */
+  int dl, dh;          /* diagonals computed: [dl, dh] */
+  long units;          /* all tiles (tiles == nullptr) */
+  const int *tiles;    /* or only these output tiles ... */
+  const int *ntiles;   /* ... *ntiles of them, counted on the device */
+  int32_t *D;          /* [nprod][P][2S-1][m][n] */
   int *err;
 };
 
 /* tensor-core phase (exact_gemm.cu): TMA maps over the digit planes and the
- * persistent tcgen05 diagonal-GEMM launch; returns an mpb_status */
-int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *err, cudaStream_t st);
+ * persistent tcgen05 diagonal-GEMM launch over diagonals [dl, dh] of every
+ * tile (tiles == nullptr) or of the device-side tile list; returns an
+ * mpb_status */
+int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *err, int dl, int dh,
+                     const int *tiles, const int *ntiles, cudaStream_t st);
 
 /* ------------------------------------------------------------------ *
  * 4. exact recombination and the single rounding
@@ -345,9 +391,18 @@ struct round_geo {
 };
 
 /* Normalise and round once: v[0..W) is the two's complement integer
- * (LSB weight 2^lsb_exp) of an exact sum; r = RNDN(v) to N limbs. */
+ * (LSB weight 2^lsb_exp) of an exact sum; r = RNDN(v) to N limbs.
+ *
+ * With cert >= 0, v is a truncated sum whose true value differs from it by
+ * less than 2^cert (LSB units), and the rounding is accepted only when every
+ * value within that distance rounds the same way: the bound must be below a
+ * quarter ULP (so no binade change can matter) and the remainder below the
+ * ULP, read as the 64-bit fraction G, must stay clear of the midpoint by
+ * more than the bound.  Returns false (r unspecified) otherwise; a zero sum
+ * is never certified. */
 template <int N, int W>
-__device__ __forceinline__ void round_words(fval<N> &r, uint32_t (&v)[W], long lsb_exp) {
+__device__ __forceinline__ bool round_words(fval<N> &r, uint32_t (&v)[W], long lsb_exp, long cert) {
+  static_assert(W >= N + 2, "word window too small");
   const uint32_t neg = v[W - 1] >> 31;
   if (neg) {
     uint32_t c = 1;
@@ -368,7 +423,7 @@ __device__ __forceinline__ void round_words(fval<N> &r, uint32_t (&v)[W], long l
   }
   if (lq == W) {
     set_zero(r);
-    return;
+    return cert < 0;
   }
   const uint32_t lr = clz32(top) & 31u;
 #pragma unroll
@@ -392,10 +447,62 @@ __device__ __forceinline__ void round_words(fval<N> &r, uint32_t (&v)[W], long l
   for (int w = 0; w < W - N - 1; ++w) st |= v[w];
   /* msb of the exact integer: 32*W - 1 - (32*lq + lr) */
   const long msb = 32L * W - 1 - (32L * lq + lr);
+  bool ok = true;
+  if (cert >= 0) {
+    const long t = cert - (msb - 32L * N + 1); /* log2 of the bound in ULPs */
+    const uint64_t G = ((uint64_t)g << 32) | v[W - N - 2];
+    const uint64_t thr = (t < -64) ? 1ull : (1ull << (64 + t)); /* >= the bound, in 2^-64 ULPs */
+    const uint64_t half = 1ull << 63;
+    ok = t <= -3 && (G <= half - thr - 1 || G > half + thr);
+  }
   int32_t ee = (int32_t)(msb + 1 + lsb_exp);
   rndn<N>(r.m, ee, g >> 31, st);
   r.e = ee;
   r.s = neg;
+  return ok;
+}
+
+/* One rounding pass of the exact GEMM (both kernels below).
+ * Pass 1 (flagged_only = 0) visits every entry, sums the diagonals
+ * [d_first, 2S-2] and, when d_first > 0, certifies the rounding against the
+ * omitted diagonals (cert); an entry that does not certify is not stored but
+ * marked in ef, and its output tile is appended once to the tile list.
+ * Pass 2 (flagged_only = 1) visits the entries of the listed tiles whose ef is
+ * set, after the tensor cores have filled in their low diagonals, and rounds
+ * the full sum (d_first = 0, no certification). */
+struct RoundPass {
+  int d_first;
+  long cert;
+  int flagged_only;
+  int nt;          /* output tiles per row of tiles */
+  uint8_t *ef;     /* m*n entry flags */
+  int *tf;         /* mt*nt tile marks */
+  int *tiles;      /* marked tiles */
+  int *ntiles;     /* their count */
+};
+
+/* entry u of a pass: false when the entry is not visited */
+__device__ __forceinline__ bool pass_entry(const RoundPass &rp, int m, int n, size_t u, int &i, int &j, size_t &idx) {
+  if (rp.flagged_only) {
+    const int tile = rp.tiles[u / (BM * BN)];
+    const int r = (int)(u % (BM * BN));
+    i = (tile / rp.nt) * BM + r / BN;
+    j = (tile % rp.nt) * BN + r % BN;
+    if (i >= m || j >= n) return false;
+    idx = (size_t)i * n + j;
+    return rp.ef[idx] != 0;
+  }
+  idx = u;
+  i = (int)(u / n);
+  j = (int)(u % n);
+  return true;
+}
+__device__ __forceinline__ size_t pass_total(const RoundPass &rp, int m, int n) {
+  return rp.flagged_only ? (size_t)(*rp.ntiles) * (BM * BN) : (size_t)m * n;
+}
+__device__ __forceinline__ void mark_tile(const RoundPass &rp, int i, int j) {
+  const int tile = (i / BM) * rp.nt + j / BN;
+  if (atomicExch(rp.tf + tile, 1) == 0) rp.tiles[atomicAdd(rp.ntiles, 1)] = tile;
 }
 
 /* Single k-part (P == 1): the diagonal planes of output idx are streamed
@@ -407,16 +514,20 @@ __device__ __forceinline__ void round_words(fval<N> &r, uint32_t (&v)[W], long l
 template <int N, int XL, bool CPLX>
 __global__ void __launch_bounds__(128) k_exact_round(int m, int n, int S, int SP, const int32_t *D,
                                                      const int32_t *rowE, const int32_t *colE, const uint8_t *rowF,
-                                                     const uint8_t *colF, uint8_t *C, size_t ldc) {
+                                                     const uint8_t *colF, uint8_t *C, size_t ldc, RoundPass rp) {
   constexpr int Q = round_geo<N, XL>::Q;
   constexpr int DMAX = 2 * round_geo<N, XL>::SMAX - 1;
-  const size_t total = (size_t)m * n, plane = (size_t)m * n;
+  const size_t total = pass_total(rp, m, n), plane = (size_t)m * n;
   const int ndiag = 2 * S - 1;
   const size_t qstride = (size_t)ndiag * plane;
-  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(idx / n), j = (int)(idx % n);
-    if (rowF[i] || colF[j]) continue; /* computed by the fallback */
+  for (size_t u = (size_t)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (size_t)gridDim.x * blockDim.x) {
+    int i, j;
+    size_t idx;
+    if (!pass_entry(rp, m, n, u, i, j, idx)) continue;
+    if (rowF[i] || colF[j]) { /* computed by the fallback */
+      if (!rp.flagged_only) rp.ef[idx] = 0;
+      continue;
+    }
     const long lsb = (long)rowE[i] + colE[j] - 2L * (32 * N) - 2L * SP;
     uint32_t vr[Q], vi[CPLX ? Q : 1];
     long long cr = 0, ci = 0;
@@ -427,7 +538,7 @@ __global__ void __launch_bounds__(128) k_exact_round(int m, int n, int S, int SP
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj) {
         const int d = 4 * w + jj;
-        if (d < DMAX && d < ndiag) {
+        if (d < DMAX && d < ndiag && d >= rp.d_first) {
           const long long scale = 1LL << (8 * jj);
           const long long t0 = __ldcs(d0 + (size_t)d * plane);
           if (CPLX) {
@@ -447,15 +558,23 @@ __global__ void __launch_bounds__(128) k_exact_round(int m, int n, int S, int SP
         ci = ti >> 32;
       }
     }
+    /* an all-zero row or column has all-zero digits: its sum is exactly 0 */
+    const long cert = (rowE[i] == kExpZero || colE[j] == kExpZero) ? -1 : rp.cert;
     fval<N> re;
-    round_words<N, Q>(re, vr, lsb);
-    if (CPLX) {
-      fval<N> im;
-      round_words<N, Q>(im, *reinterpret_cast<uint32_t(*)[Q]>(vi), lsb);
-      store_celem<N>(C, (size_t)i * ldc + j, re, im);
-    } else {
-      store_elem<N>(C, (size_t)i * ldc + j, re);
+    bool ok = round_words<N, Q>(re, vr, lsb, cert);
+    fval<N> im;
+    if (CPLX) ok = round_words<N, Q>(im, *reinterpret_cast<uint32_t(*)[Q]>(vi), lsb, cert) && ok;
+    if (!rp.flagged_only) {
+      rp.ef[idx] = ok ? 0 : 1;
+      if (!ok) {
+        mark_tile(rp, i, j);
+        continue;
+      }
     }
+    if (CPLX)
+      store_celem<N>(C, (size_t)i * ldc + j, re, im);
+    else
+      store_elem<N>(C, (size_t)i * ldc + j, re);
   }
 }
 
@@ -466,16 +585,23 @@ template <int N, int XL, bool CPLX>
 __global__ void __launch_bounds__(128) k_exact_round_parts(int m, int n, int S, int SP, int P, const int32_t *D,
                                                            const int32_t *rowE, const int32_t *colE,
                                                            const uint8_t *rowF, const uint8_t *colF, uint8_t *C,
-                                                           size_t ldc) {
+                                                           size_t ldc, RoundPass rp) {
   constexpr int Q = round_geo<N, XL>::Q;
-  const size_t total = (size_t)m * n, plane = (size_t)m * n;
+  const size_t total = pass_total(rp, m, n), plane = (size_t)m * n;
   const int ndiag = 2 * S - 1;
   const size_t pstride = (size_t)ndiag * plane, qstride = (size_t)P * pstride;
-  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(idx / n), j = (int)(idx % n);
-    if (rowF[i] || colF[j]) continue;
+  for (size_t u = (size_t)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (size_t)gridDim.x * blockDim.x) {
+    int i, j;
+    size_t idx;
+    if (!pass_entry(rp, m, n, u, i, j, idx)) continue;
+    if (rowF[i] || colF[j]) {
+      if (!rp.flagged_only) rp.ef[idx] = 0;
+      continue;
+    }
     const long lsb = (long)rowE[i] + colE[j] - 2L * (32 * N) - 2L * SP;
+    const long cert = (rowE[i] == kExpZero || colE[j] == kExpZero) ? -1 : rp.cert;
+    fval<N> res[CPLX ? 2 : 1];
+    bool ok = true;
 #pragma unroll 1
     for (int comp = 0; comp < (CPLX ? 2 : 1); ++comp) {
       /* coefficients of T0, T1, T2 for this component */
@@ -485,7 +611,7 @@ __global__ void __launch_bounds__(128) k_exact_round_parts(int m, int n, int S, 
       long long acc[Q];
       for (int w = 0; w < Q; ++w) acc[w] = 0;
 #pragma unroll 1
-      for (int d = 0; d < ndiag; ++d) {
+      for (int d = rp.d_first; d < ndiag; ++d) {
         long long s = 0;
 #pragma unroll 1
         for (int p = 0; p < P; ++p) {
@@ -504,16 +630,20 @@ __global__ void __launch_bounds__(128) k_exact_round_parts(int m, int n, int S, 
         v[w] = (uint32_t)t;
         carry = t >> 32;
       }
-      fval<N> r;
-      round_words<N, Q>(r, v, lsb);
-      const size_t e = (size_t)i * ldc + j;
-      if (CPLX) {
-        uint8_t *ct = C + (e >> 5) * 2u * sol<N>::kTileBytes + (size_t)comp * sol<N>::kTileBytes;
-        store_elem<N>(ct, e & 31u, r);
-      } else {
-        store_elem<N>(C, e, r);
+      ok = round_words<N, Q>(res[comp], v, lsb, cert) && ok;
+    }
+    if (!rp.flagged_only) {
+      rp.ef[idx] = ok ? 0 : 1;
+      if (!ok) {
+        mark_tile(rp, i, j);
+        continue;
       }
     }
+    const size_t e = (size_t)i * ldc + j;
+    if (CPLX)
+      store_celem<N>(C, e, res[0], res[CPLX ? 1 : 0]);
+    else
+      store_elem<N>(C, e, res[0]);
   }
 }
 
@@ -558,10 +688,21 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
                     size_t ldc, uint8_t *ws, int *n_fallback, cudaStream_t st) {
   int32_t *rowE = (int32_t *)(ws + p.off_rowE), *colE = (int32_t *)(ws + p.off_colE);
   uint8_t *rowF = ws + p.off_flags, *colF = ws + p.off_flags + p.m;
-  int *cnt = (int *)(ws + p.off_cnt); /* [0] fallback rows+cols, [1] kernel error code */
+  int *cnt = (int *)(ws + p.off_cnt); /* [0] fallback rows+cols, [1] kernel error code, [2] marked tiles */
   int8_t *Asl = (int8_t *)(ws + p.off_asl), *Bsl = (int8_t *)(ws + p.off_bsl);
   int32_t *D = (int32_t *)(ws + p.off_d);
-  if (cudaMemsetAsync(cnt, 0, 16, st) != cudaSuccess) return MPB_ERR_CUDA;
+  RoundPass rp;
+  rp.d_first = p.d0;
+  rp.cert = p.cert;
+  rp.flagged_only = 0;
+  rp.nt = p.nt;
+  rp.ef = ws + p.off_ef;
+  rp.tf = (int *)(ws + p.off_tf);
+  rp.tiles = (int *)(ws + p.off_tiles);
+  rp.ntiles = cnt + 2;
+  if (cudaMemsetAsync(cnt, 0, 16, st) != cudaSuccess ||
+      cudaMemsetAsync(rp.tf, 0, 4 * (size_t)p.mt * p.nt, st) != cudaSuccess)
+    return MPB_ERR_CUDA;
 
   profile_mark(kPhaseStats, true, st);
   k_row_stats<N, CPLX><<<(p.m + 7) / 8, 256, 0, st>>>(p.m, p.k, A, lda, p.SP, rowE, rowF, cnt);
@@ -579,21 +720,36 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
   profile_mark(kPhaseSlice, false, st);
   if (launch_status() != MPB_OK) return MPB_ERR_CUDA;
 
+  /* main pass: diagonals [d0, 2S-2] of every tile */
   {
-    const int rc = launch_diag_gemm(p, Asl, Bsl, D, cnt + 1, st);
+    const int rc = launch_diag_gemm(p, Asl, Bsl, D, cnt + 1, p.d0, 2 * p.S - 2, nullptr, nullptr, st);
     if (rc != MPB_OK) return rc;
   }
-
+  auto round_pass = [&](const RoundPass &r, int grid_cap) {
+    if (p.P == 1) {
+      const int g = std::min(grid_cap, grid_for(k_exact_round<N, XL, CPLX>, 128, (size_t)p.m * p.n));
+      k_exact_round<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.n, p.S, p.SP, D, rowE, colE, rowF, colF, C, ldc, r);
+    } else {
+      const int g = std::min(grid_cap, grid_for(k_exact_round_parts<N, XL, CPLX>, 128, (size_t)p.m * p.n));
+      k_exact_round_parts<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.n, p.S, p.SP, p.P, D, rowE, colE, rowF, colF, C,
+                                                          ldc, r);
+    }
+  };
   profile_mark(kPhaseRound, true, st);
-  if (p.P == 1) {
-    const int g = grid_for(k_exact_round<N, XL, CPLX>, 128, (size_t)p.m * p.n);
-    k_exact_round<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.n, p.S, p.SP, D, rowE, colE, rowF, colF, C, ldc);
-  } else {
-    const int g = grid_for(k_exact_round_parts<N, XL, CPLX>, 128, (size_t)p.m * p.n);
-    k_exact_round_parts<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.n, p.S, p.SP, p.P, D, rowE, colE, rowF, colF, C,
-                                                        ldc);
-  }
+  round_pass(rp, 1 << 30);
   profile_mark(kPhaseRound, false, st);
+  if (p.d0 > 0) {
+    /* tiles holding an entry that did not certify: low diagonals on the
+     * tensor cores, then the full sum for those entries (the tile count is
+     * read on the device; with no marked tile both launches return at once) */
+    const int rc = launch_diag_gemm(p, Asl, Bsl, D, cnt + 1, 0, p.d0 - 1, rp.tiles, rp.ntiles, st);
+    if (rc != MPB_OK) return rc;
+    RoundPass r2 = rp;
+    r2.d_first = 0;
+    r2.cert = -1;
+    r2.flagged_only = 1;
+    round_pass(r2, 4 * sm_count());
+  }
   profile_mark(kPhaseFallback, true, st);
   {
     const dim3 grid((p.n + 31) / 32, (p.m + 7) / 8);

@@ -71,11 +71,15 @@ def test_empty_inputs_are_noops(mpb):
 
 def test_exact_gemm_workspace_and_checks(mpb):
     L = mpb.lib()
-    # PB=512, 1024^3, 32-bit spread: S = 69 digit planes, 137 diagonals
+    # PB=512, 1024^3, 32-bit spread: S = 69 digit planes, 137 diagonals, plus
+    # one certification flag byte per entry
     S, m = 69, 1024
     need = L.mpb_gemm_exact_workspace(512, m, m, m, 32)
-    planes = S * 2 * m * m + 137 * m * m * 4
+    planes = S * 2 * m * m + 137 * m * m * 4 + m * m
     assert planes <= need <= planes + 64 * 1024
+    # the tensor cores skip the low diagonals 0..62: 2745 of the 69^2 slice pairs
+    assert mpb.gemm_exact_info(512, m, m, m, 32) == (69, 63, 2745)
+    assert mpb.gemm_exact_info(256, 512, 512, 512, 16, cplx=True) == (35, 27, 847)
     assert L.mpb_gemm_exact_workspace(96, 8, 8, 8, 32) == 0
     good = 4096
     # missing workspace, misaligned workspace, bad leading dimension
@@ -90,7 +94,7 @@ def test_exact_gemm_complex_workspace(mpb):
     # PB=256, 512^3 complex, 16-bit spread: S = ceil((256+16+3)/8) = 35, 3 products
     S, m = 35, 512
     need = L.mpb_gemm_exact_c_workspace(256, m, m, m, 16)
-    planes = 3 * S * 2 * m * m + 3 * (2 * S - 1) * m * m * 4
+    planes = 3 * S * 2 * m * m + 3 * (2 * S - 1) * m * m * 4 + m * m
     assert planes <= need <= planes + 64 * 1024
     assert L.mpb_gemm_exact_c(256, 8, 8, 8, 4096, 32, 4096, 32, 4096, 32, 16, None, 0, None, None) == -8
 

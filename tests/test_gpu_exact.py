@@ -74,6 +74,45 @@ def test_exact_cancellation_and_signs(orc, mpb, prec):
     assert orc.mismatches(prec, C, exp)[0] == 0
 
 
+@pytest.mark.parametrize("prec", (128, 512))
+def test_exact_uncertified_entries_are_recomputed(orc, mpb, prec):
+    """Sums that cancel inside the dot product: the tensor cores skip the
+    low-order slice pairs, so these entries cannot certify their rounding
+    from the truncated sum and must be recomputed from the full sum.
+
+    A = [H, H'] and, for the columns in J, B = [G; -G]: every such entry is
+    exactly 0 (H' = H) or a residual ~2^-PB below its terms (rows in I, where
+    H' differs from H in the last bit of one entry).  The other columns are
+    ordinary random sums.  m, n span two output tiles each, so marked and
+    unmarked tiles mix."""
+    m, n, k = 130, 300, 96
+    h = k // 2
+    rng = np.random.default_rng(prec)
+    H = rand_aos(prec, m * h, 31, -4, 4, 0.0).reshape(m, h, -1)
+    H2 = H.copy()
+    rows_i = rng.choice(m, 40, replace=False)
+    H2[rows_i, 0, 16] ^= 1  # lowest limb byte of entry (i, h): last significand bit
+    A = np.concatenate([H, H2], axis=1).reshape(m * k, -1)
+    G = rand_aos(prec, h * n, 32, -4, 4, 0.0).reshape(h, n, -1)
+    negG = G.copy()
+    negG[:, :, 0:4] = (-negG[:, :, 0:4].view(np.int32)).view(np.uint8)
+    B = np.concatenate([G, rand_aos(prec, h * n, 33, -4, 4, 0.0).reshape(h, n, -1)], axis=0)
+    cols_j = rng.choice(n, 120, replace=False)
+    B[h:, cols_j] = negG[:, cols_j]
+    B = B.reshape(k * n, -1)
+    C, st = run_exact(mpb, prec, m, n, k, A, B, sp_bits=16)
+    assert st[1] == 0 and st[0] == 0
+    exp = orc.gemm_exact(prec, m, n, k, A, k, B, n, impl="mp")
+    bad, first = orc.mismatches(prec, C, exp)
+    assert bad == 0, f"PB={prec}: {bad} mismatches, first at {first}"
+    # the construction really produced exact zeros and deep cancellation
+    Cm = C.reshape(m, n, -1)
+    zero_exp = layout.AOS_ZERO_EXP
+    ez = Cm[:, cols_j, 8:16].copy().view(np.int64).reshape(m, len(cols_j))
+    others = np.setdiff1d(np.arange(m), rows_i)
+    assert (ez[others] == zero_exp).all() and (ez[rows_i] != zero_exp).all()
+
+
 def test_exact_fallback_rows_and_columns(orc, mpb):
     """Rows/columns whose exponent spread exceeds the budget take the plain
     per-operation-rounded kernel (never the CPU) and are counted."""
