@@ -297,8 +297,15 @@ class GemmWorkload:
     def default_steps(self):
         return 2000 if self.cplx else 200  # ~1 s of GPU time: long enough for clock sampling
 
-    launches_per_step = 7  # stats x2, slice x2, tensor-core GEMM, round, fallback
-    e2e_launches_per_step = 10
+    @property
+    def launches_per_step(self):
+        # stats x2, slice x2, tensor-core GEMM, round, fallback; with truncated
+        # diagonals also the (usually empty) low-diagonal GEMM and second round
+        return 7 + (2 if getattr(self, "d0", 0) > 0 else 0)
+
+    @property
+    def e2e_launches_per_step(self):
+        return self.launches_per_step + 3  # + pack A, pack B, unpack C
 
     def make_host(self, rank):
         from mpc_cuda_b200 import layout
