@@ -87,6 +87,9 @@ int mpb_to_double(int prec, size_t n, const void *vec, double *d, void *stream);
 int mpb_binop_r(int prec, int op, size_t n, const void *a, const void *b, void *r, void *stream);
 /* r[i] = round(a[i]*b[i] + c[i]), one rounding (mpfr_fma; no counterpart in the reference) */
 int mpb_fma_r(int prec, size_t n, const void *a, const void *b, const void *c, void *r, void *stream);
+/* complex r[i] = a[i]*b[i] + c[i], one rounding per component from exact
+ * products (mpc_fma; the drop-in cu_cfma; no counterpart in the reference) */
+int mpb_fma_c(int prec, size_t n, const void *a, const void *b, const void *c, void *r, void *stream);
 /* complex r[i] = a[i] op b[i] (reference cu_cmul/cu_cadd/cu_csub, cu_fcomplex.cuh:115-131) */
 int mpb_binop_c(int prec, int op, size_t n, const void *a, const void *b, void *r, void *stream);
 

@@ -15,6 +15,7 @@
  *   add_round    round(x + y)              (x, y exact NX-limb terms, result NM limbs)
  *   fma          round(a*b + c)            (single rounding)
  *   fmms/fmma    round(a*b -/+ c*d)        (single rounding; complex multiply)
+ *   sum3_round   round(t1 + t2 + t3)       (three exact terms; complex fma: cfma)
  * Zero is unsigned (+0), as in cu_freal (cu_freal.cuh:79-81 of mpc_cuda).
  *
  * B200 design points:
@@ -462,6 +463,208 @@ MPB_HD void cmul(fval<N> &rr, fval<N> &ri, const fval<N> &ar, const fval<N> &ai,
                  const fval<N> &br, const fval<N> &bi) {
   fmms<N, kVote>(rr, ar, br, ai, bi, 1u);
   fmms<N, kVote>(ri, ar, bi, ai, br, 0u);
+}
+
+/* ------------------------------------------------------------------ *
+ * r = round(t1 + t2 + t3) for three exact terms, one rounding.
+ * ------------------------------------------------------------------ */
+/* Window sum of two exact L-limb terms: x (the larger exponent; zero only if
+ * y is zero too) sits in the top L of WS = 2L + 2 words, y is shifted right
+ * by d = xe - ye.  When d <= 32 (L + 1) every bit of y lands in words 1..WS-1
+ * and the sum is exact; otherwise the bits of y below the window become the
+ * sticky-borrow of add_round and are folded into the lowest bit, which makes
+ * the sum round-to-odd at 32 WS bits.  o is normalised (top bit set), zero is
+ * kExpZero with zero words.  Exponents follow add_round: the alignment shift
+ * of two terms is their exponent difference. */
+template <int L>
+MPB_HD void sum2_odd(uint32_t (&o)[2 * L + 2], int32_t &oe, uint32_t &os, const uint32_t *xm, int32_t xe,
+                     uint32_t xs, const uint32_t *ym, int32_t ye, uint32_t ys) {
+  constexpr int WS = 2 * L + 2;
+  constexpr int KQ = log2_ceil<WS + 1>::v;
+  uint32_t D[WS + 1], Y[WS];
+  MPB_UNROLL
+  for (int i = 0; i < WS; ++i) {
+    D[i] = (i >= WS - L) ? xm[i - (WS - L)] : 0u;
+    Y[i] = (i >= WS - L) ? ym[i - (WS - L)] : 0u;
+  }
+  const uint32_t d = (uint32_t)(xe - ye);
+  const uint32_t q = (d >> 5) < (uint32_t)WS ? (d >> 5) : (uint32_t)WS;
+  const uint32_t rs = d & 31u;
+  uint32_t st = 0u;
+  MPB_UNROLL
+  for (int k = 0; k < KQ; ++k) {
+    const int sh = 1 << k;
+    const bool on = (q >> k) & 1u;
+    uint32_t lost = 0u;
+    MPB_UNROLL
+    for (int i = 0; i < sh && i < WS; ++i) lost |= Y[i];
+    st |= on ? lost : 0u;
+    MPB_UNROLL
+    for (int i = 0; i < WS; ++i) {
+      const uint32_t src = (i + sh < WS) ? Y[i + sh] : 0u;
+      Y[i] = on ? src : Y[i];
+    }
+  }
+  st |= Y[0] & ((1u << rs) - 1u);
+  MPB_UNROLL
+  for (int i = 0; i < WS - 1; ++i) Y[i] = fshr(Y[i], Y[i + 1], rs);
+  Y[WS - 1] >>= rs;
+
+  const uint32_t sub = xs ^ ys;
+  const uint32_t msk = 0u - sub;
+  uint32_t cf = 0;
+  cc_set(sub & (st == 0u ? 1u : 0u), cf);
+  MPB_UNROLL
+  for (int i = 0; i < WS; ++i) D[i] = addc_cc(D[i], Y[i] ^ msk, cf);
+  const uint32_t c = addc(0u, 0u, cf);
+  const uint32_t neg = sub & (c ^ 1u); /* only when d == 0: exact negation */
+  {
+    const uint32_t nm = 0u - neg;
+    uint32_t cf2 = 0;
+    cc_set(neg, cf2);
+    MPB_UNROLL
+    for (int i = 0; i < WS; ++i) D[i] = addc_cc(D[i] ^ nm, 0u, cf2);
+  }
+  const uint32_t cs = (sub ^ 1u) & c;
+  st |= D[0] & cs;
+  D[WS] = c;
+  MPB_UNROLL
+  for (int i = 0; i < WS; ++i) D[i] = fshr(D[i], D[i + 1], cs);
+  D[0] |= (st != 0u) ? 1u : 0u; /* round to odd */
+
+  uint32_t lq = (uint32_t)WS, top = 0u;
+  MPB_UNROLL
+  for (int i = WS - 1; i >= 0; --i) {
+    const bool take = (lq == (uint32_t)WS) && (D[i] != 0u);
+    top = take ? D[i] : top;
+    lq = take ? (uint32_t)(WS - 1 - i) : lq;
+  }
+  const bool zero = (lq == (uint32_t)WS);
+  const uint32_t lr = clz32(top) & 31u;
+  const uint32_t qq = zero ? 0u : lq;
+  MPB_UNROLL
+  for (int k = 0; k < KQ; ++k) {
+    const int sh = 1 << k;
+    const bool on = (qq >> k) & 1u;
+    MPB_UNROLL
+    for (int i = WS - 1; i >= 0; --i) {
+      const uint32_t src = (i - sh >= 0) ? D[i - sh] : 0u;
+      D[i] = on ? src : D[i];
+    }
+  }
+  MPB_UNROLL
+  for (int i = WS - 1; i > 0; --i) D[i] = fshl(D[i - 1], D[i], lr);
+  D[0] <<= lr;
+  MPB_UNROLL
+  for (int i = 0; i < WS; ++i) o[i] = zero ? 0u : D[i];
+  oe = zero ? kExpZero : xe + (int32_t)cs - (int32_t)(32u * lq + lr);
+  os = zero ? 0u : (xs ^ neg);
+}
+
+/* round(t1 + t2 + t3), each term exact with L limbs (normalised or zero).
+ * With the terms ordered by exponent: if the second fits the window of the
+ * first (gap <= 32 (L + 1) bits), their sum is exact and is rounded together
+ * with the third by add_round; otherwise the first term is more than 32(L+1)
+ * bits above the other two, their window sum is rounded to odd at 32(2L+2)
+ * bits -- its last bit lies below add_round's window, where only the sign
+ * and the non-zeroness of the remainder matter, and rounding to odd keeps
+ * both -- and it is rounded together with the first. */
+template <int L, int NM, bool kVote = false>
+MPB_HD void sum3_round(fval<NM> &r, const uint32_t *am, int32_t ae, uint32_t as, const uint32_t *bm, int32_t be,
+                       uint32_t bs, const uint32_t *cm, int32_t ce, uint32_t cs) {
+  constexpr int WS = 2 * L + 2;
+  /* order by exponent: t1 >= t2 >= t3 (selects, no runtime-indexed arrays) */
+  uint32_t t1[L], t2[L], t3[L];
+  int32_t e1 = ae, e2 = be, e3 = ce;
+  uint32_t s1 = as, s2 = bs, s3 = cs;
+  MPB_UNROLL
+  for (int i = 0; i < L; ++i) {
+    t1[i] = am[i];
+    t2[i] = bm[i];
+    t3[i] = cm[i];
+  }
+  auto cswap = [&](uint32_t(&x)[L], int32_t &xe, uint32_t &xs, uint32_t(&y)[L], int32_t &ye, uint32_t &ys) {
+    const bool sw = ye > xe;
+    MPB_UNROLL
+    for (int i = 0; i < L; ++i) {
+      const uint32_t a = x[i], b = y[i];
+      x[i] = sw ? b : a;
+      y[i] = sw ? a : b;
+    }
+    const int32_t ea = xe, eb = ye;
+    xe = sw ? eb : ea;
+    ye = sw ? ea : eb;
+    const uint32_t sa = xs, sb = ys;
+    xs = sw ? sb : sa;
+    ys = sw ? sa : sb;
+  };
+  cswap(t1, e1, s1, t2, e2, s2);
+  cswap(t2, e2, s2, t3, e3, s3);
+  cswap(t1, e1, s1, t2, e2, s2);
+
+  /* near: sum t1 + t2 exactly, then round with t3; far: t2 + t3 (exact or
+   * rounded to odd), then round with t1 -- one window sum either way */
+  const bool near = (int64_t)e1 - e2 <= 32 * (L + 1);
+  uint32_t P[L], Q[L], X[WS], S[WS];
+  MPB_UNROLL
+  for (int i = 0; i < L; ++i) {
+    P[i] = near ? t1[i] : t2[i];
+    Q[i] = near ? t2[i] : t3[i];
+  }
+  MPB_UNROLL
+  for (int i = 0; i < WS; ++i) X[i] = (i >= WS - L) ? (near ? t3[i - (WS - L)] : t1[i - (WS - L)]) : 0u;
+  int32_t se;
+  uint32_t ss;
+  sum2_odd<L>(S, se, ss, P, near ? e1 : e2, near ? s1 : s2, Q, near ? e2 : e3, near ? s2 : s3);
+  add_round<WS, NM, kVote>(r, X, near ? e3 : e1, near ? s3 : s1, S, se, ss);
+}
+
+/* round(a*b + c*d + e) with one rounding (negate_cd flips the sign of c*d):
+ * one component of a complex fused multiply-add */
+template <int N, bool kVote = false>
+MPB_HD void fmma_add(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c, const fval<N> &d,
+                     const fval<N> &e, uint32_t negate_cd) {
+  uint32_t p1[2 * N], p2[2 * N], ew[2 * N];
+  int32_t e1, e2;
+  mul_exact_norm<N>(p1, e1, a, b);
+  mul_exact_norm<N>(p2, e2, c, d);
+  MPB_UNROLL
+  for (int i = 0; i < N; ++i) {
+    ew[i] = 0u;
+    ew[N + i] = e.m[i];
+  }
+  const uint32_t s2 = (e2 == kExpZero) ? 0u : (c.s ^ d.s ^ negate_cd);
+  sum3_round<2 * N, N, kVote>(r, p1, e1, (e1 == kExpZero) ? 0u : (a.s ^ b.s), p2, e2, s2, ew, e.e, e.s);
+}
+
+/* complex (MPC_RNDNN) fused multiply-add: re = round(ar*br - ai*bi + cr),
+ * im = round(ar*bi + ai*br + ci), each with one rounding (MPC mpc_fma).  The
+ * two components run through one instance of the three-term sum (a loop
+ * over the component with selected operands) to halve the code. */
+template <int N, bool kVote = false>
+MPB_HD void cfma(fval<N> &rr, fval<N> &ri, const fval<N> &ar, const fval<N> &ai, const fval<N> &br,
+                 const fval<N> &bi, const fval<N> &cr, const fval<N> &ci) {
+#ifdef __CUDA_ARCH__
+#pragma unroll 1
+#endif
+  for (int comp = 0; comp < 2; ++comp) {
+    const bool im = comp == 1;
+    fval<N> y, z, r;
+    MPB_UNROLL
+    for (int i = 0; i < N; ++i) {
+      y.m[i] = im ? bi.m[i] : br.m[i];
+      z.m[i] = im ? br.m[i] : bi.m[i];
+    }
+    y.e = im ? bi.e : br.e;
+    y.s = im ? bi.s : br.s;
+    z.e = im ? br.e : bi.e;
+    z.s = im ? br.s : bi.s;
+    fmma_add<N, kVote>(r, ar, y, ai, z, im ? ci : cr, im ? 0u : 1u);
+    if (im)
+      ri = r;
+    else
+      rr = r;
+  }
 }
 
 /* magnitude / signed compare (-1, 0, 1) */

@@ -6,7 +6,8 @@
  * The complex product rounds each component once from exact products:
  *   re = round(ar*br - ai*bi),  im = round(ar*bi + ai*br)
  * computed by the mpb core (mpb::fmms): two exact 2N-limb products and one
- * aligned sum in registers, no intermediate rounding.
+ * aligned sum in registers, no intermediate rounding.  Added over the
+ * reference: cu_cfma (a*b + c, one rounding per component, MPC mpc_fma).
  */
 #ifndef MPB_DROPIN_CU_FCOMPLEX_CUH
 #define MPB_DROPIN_CU_FCOMPLEX_CUH
@@ -145,6 +146,22 @@ __host__ __device__ static inline cu_fcomplex<PB> operator-(const cu_fcomplex<PB
 template <int PB>
 __host__ __device__ static inline cu_fcomplex<PB> operator*(const cu_fcomplex<PB> &a, const cu_fcomplex<PB> &b) {
   return cu_cmul<PB>(a, b);
+}
+/* a*b + c with one rounding per component (MPC mpc_fma semantics; not in
+ * the reference): re = round(ar*br - ai*bi + cr), im = round(ar*bi + ai*br + ci)
+ * from exact products */
+template <int PB>
+__host__ __device__ static inline cu_fcomplex<PB> cu_cfma(const cu_fcomplex<PB> &a, const cu_fcomplex<PB> &b,
+                                                          const cu_fcomplex<PB> &c) {
+  typename detail::core_of<PB>::type ar, ai, br, bi, cr, ci, rr, ri;
+  detail::to_core<PB>(ar, a.re);
+  detail::to_core<PB>(ai, a.im);
+  detail::to_core<PB>(br, b.re);
+  detail::to_core<PB>(bi, b.im);
+  detail::to_core<PB>(cr, c.re);
+  detail::to_core<PB>(ci, c.im);
+  mpb::cfma(rr, ri, ar, ai, br, bi, cr, ci);
+  return cu_fcomplex<PB>(detail::from_core<PB>(rr), detail::from_core<PB>(ri));
 }
 
 } /* namespace cu_fp */

@@ -57,6 +57,7 @@ _SIGS = {
     "mpb_to_double": ([_I, _S, _V, _V, _V], C.c_int),
     "mpb_binop_r": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
     "mpb_fma_r": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
+    "mpb_fma_c": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
     "mpb_binop_c": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
     "mpb_axpy_r": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
     "mpb_axpy_c": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
@@ -119,6 +120,7 @@ def host_lib():
         for name in ("mpbh_binop", "mpbh_cbinop"):
             getattr(H, name).argtypes = [_I, _I, _L, _V, _V, _V]
         H.mpbh_fma.argtypes = [_I, _L, _V, _V, _V, _V]
+        H.mpbh_cfma.argtypes = [_I, _L, _V, _V, _V, _V]
         for name in ("mpbh_axpy_r", "mpbh_axpy_c"):
             getattr(H, name).argtypes = [_I, _L, _V, _V, _V, _V]
         H.mpbh_from_double.argtypes = [_I, _L, _V, _V]
@@ -199,8 +201,9 @@ def binop(prec, op, n, a, b, r, cplx=False, stream=None):
     _call("mpb_binop_c" if cplx else "mpb_binop_r", prec, op, n, _ptr(a), _ptr(b), _ptr(r), _stream(stream))
 
 
-def fma(prec, n, a, b, c, r, stream=None):
-    _call("mpb_fma_r", prec, n, _ptr(a), _ptr(b), _ptr(c), _ptr(r), _stream(stream))
+def fma(prec, n, a, b, c, r, cplx=False, stream=None):
+    """r = a*b + c with one rounding (per component when complex)."""
+    _call("mpb_fma_c" if cplx else "mpb_fma_r", prec, n, _ptr(a), _ptr(b), _ptr(c), _ptr(r), _stream(stream))
 
 
 def axpy(prec, n, a, x, y, z, cplx=False, stream=None):

@@ -337,6 +337,7 @@ extern "C" int mpb_to_double(int prec, size_t n, const void *vec, double *d, voi
   return launch_status();
 }
 
+
 static int vec_args(int prec, size_t n, std::initializer_list<const void *> bufs) {
   if (!prec_ok(prec)) return MPB_ERR_PREC;
   if (n > kMaxElems) return MPB_ERR_SIZE;

@@ -12,6 +12,7 @@
  *   mpbh_binop(prec, op, n, a, b, r)     op 0 mul, 1 add, 2 sub
  *   mpbh_fma(prec, n, a, b, c, r)
  *   mpbh_cbinop(prec, op, n, a, b, r)    op 0 cmul, 1 cadd, 2 csub
+ *   mpbh_cfma(prec, n, a, b, c, r)       cu_cfma
  *   mpbh_axpy_r / mpbh_axpy_c(prec, n, a, x, y, z)
  *   mpbh_from_double / mpbh_to_double(prec, n, ...)
  * Return 0, or -1 for an unsupported precision.
@@ -48,6 +49,15 @@ void fma3(long n, const void *A, const void *B, const void *C, void *R) {
   auto r = (cu_freal<PB> *)R;
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < n; i++) r[i] = cu_fp::cu_ffma<PB>(a[i], b[i], c[i]);
+}
+template <int PB>
+void cfma3(long n, const void *A, const void *B, const void *C, void *R) {
+  auto a = (const cu_fcomplex<PB> *)A;
+  auto b = (const cu_fcomplex<PB> *)B;
+  auto c = (const cu_fcomplex<PB> *)C;
+  auto r = (cu_fcomplex<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_cfma<PB>(a[i], b[i], c[i]);
 }
 template <int PB>
 void cbinop(int op, long n, const void *A, const void *B, void *R) {
@@ -120,6 +130,9 @@ int mpbh_fma(int prec, long n, const void *a, const void *b, const void *c, void
 }
 int mpbh_cbinop(int prec, int op, long n, const void *a, const void *b, void *r) {
   MPBH_DISPATCH(prec, cbinop<PB>(op, n, a, b, r))
+}
+int mpbh_cfma(int prec, long n, const void *a, const void *b, const void *c, void *r) {
+  MPBH_DISPATCH(prec, cfma3<PB>(n, a, b, c, r))
 }
 int mpbh_axpy_r(int prec, long n, const void *a, const void *x, const void *y, void *z) {
   MPBH_DISPATCH(prec, axpy_r<PB>(n, a, x, y, z))

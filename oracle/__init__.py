@@ -54,7 +54,7 @@ def lib():
         for name in ("orc_mul", "orc_add", "orc_sub", "orc_cmul", "orc_cadd", "orc_csub",
                      "mp_mul", "mp_add", "mp_sub", "mp_cmul", "mp_cadd", "mp_csub"):
             getattr(L, name).argtypes = [it, lg, vp, vp, vp]
-        for name in ("orc_fma", "mp_fma"):
+        for name in ("orc_fma", "mp_fma", "mp_cfma", "mp_cfma_dot"):
             getattr(L, name).argtypes = [it, lg, vp, vp, vp, vp]
         for name in ("orc_axpy_r", "orc_axpy_c", "mp_axpy_r", "mp_axpy_c"):
             getattr(L, name).argtypes = [it, lg, vp, vp, vp, vp]
@@ -151,9 +151,17 @@ def binop(kind: str, prec: int, A: np.ndarray, B: np.ndarray, impl: str = "orc")
     return R
 
 
-def fma(prec: int, A, B, Cc, impl: str = "orc") -> np.ndarray:
-    R = empty(prec, A.shape[0])
-    getattr(lib(), f"{impl}_fma")(prec, A.shape[0], _p(A), _p(B), _p(Cc), _p(R))
+def fma(prec: int, A, B, Cc, impl: str = "orc", cplx: bool = False) -> np.ndarray:
+    """a*b + c, one rounding (per component).  Complex: impl 'mp' = mpc_fma,
+    'mpdot' = mpc_dot over ([a, c], [b, 1]); the reference has no fma."""
+    R = empty(prec, A.shape[0], cplx)
+    if cplx:
+        if impl not in ("mp", "mpdot"):
+            raise ValueError("complex fma: impl 'mp' or 'mpdot'")
+        name = "mp_cfma_dot" if impl == "mpdot" else "mp_cfma"
+    else:
+        name = f"{impl}_fma"
+    getattr(lib(), name)(prec, A.shape[0], _p(A), _p(B), _p(Cc), _p(R))
     return R
 
 

@@ -1001,6 +1001,45 @@ void mp_cmul(int P, long n, const void *A, const void *B, void *R) { mp_cbin(mpc
 void mp_cadd(int P, long n, const void *A, const void *B, void *R) { mp_cbin(mpc_add, P, n, A, B, R); }
 void mp_csub(int P, long n, const void *A, const void *B, void *R) { mp_cbin(mpc_sub, P, n, A, B, R); }
 
+/* complex fused multiply-add a*b + c, one rounding per component: the
+ * system mpc_fma, and independently mpc_dot over ([a, c], [b, 1]); the
+ * reference has no such operation (checker for the engine's cu_cfma) */
+void mp_cfma(int P, long n, const void *A, const void *B, const void *C, void *R) {
+  size_t es = 2 * esz_of(P);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    shim_mpc_t a, b, c, r;
+    as_mpc(P, a, cat(A, es, i));
+    as_mpc(P, b, cat(B, es, i));
+    as_mpc(P, c, cat(C, es, i));
+    mpc_init2(r, P); /* an ordinary destination: the library may swap significands */
+    mpc_fma(r, a, b, c, SHIM_MPC_RNDNN);
+    store_mpfr(P, RE(at(R, es, i)), r->re);
+    store_mpfr(P, IM(at(R, es, i), esz_of(P)), r->im);
+    mpc_clear(r);
+  }
+}
+void mp_cfma_dot(int P, long n, const void *A, const void *B, const void *C, void *R) {
+  size_t es = 2 * esz_of(P);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    shim_mpc_t a, b, c, one, r;
+    as_mpc(P, a, cat(A, es, i));
+    as_mpc(P, b, cat(B, es, i));
+    as_mpc(P, c, cat(C, es, i));
+    mpc_init2(one, 64);
+    mpfr_set_d(one->re, 1.0, SHIM_RNDN);
+    mpfr_set_d(one->im, 0.0, SHIM_RNDN);
+    mpc_init2(r, P);
+    shim_mpc_ptr x[2] = {a, c}, y[2] = {b, one};
+    mpc_dot(r, x, y, 2, SHIM_MPC_RNDNN);
+    store_mpfr(P, RE(at(R, es, i)), r->re);
+    store_mpfr(P, IM(at(R, es, i), esz_of(P)), r->im);
+    mpc_clear(r);
+    mpc_clear(one);
+  }
+}
+
 /* real AXPY via MPFR, the call sequence of cpu_axpy_real
  * (demos/bench3_cpu.cpp:35-57: mul then add, RNDN, OpenMP static) with the
  * operands bound in place instead of mpfr_set_d.  Each thread owns its

@@ -71,6 +71,26 @@ def test_binops_complex(orc, mpb, prec):
         assert bad == 0, f"{kind} PB={prec}: {bad} mismatches, first at {first}"
 
 
+@pytest.mark.parametrize("prec", PRECS)
+def test_fma_complex(orc, mpb, prec):
+    """mpb_fma_c (the drop-in cu_cfma): one rounding per component, against the
+    system mpc_fma, on the reference generator's wide-spread pairs and on
+    c = -round(a*b), whose sums cancel down to the product's rounding error."""
+    M = 20000 if prec <= 1024 else 4000
+    A, B = orc.gen_pairs(prec, M, 0xCF + prec, cplx=True)
+    Cc, _ = orc.gen_pairs(prec, M, 0xFC + prec, cplx=True)
+    a, b, r = dvec(prec, A, True), dvec(prec, B, True), mpb.empty(prec, M, True)
+    AB = orc.binop("cmul", prec, A, B, "mp")
+    es = layout.aos_bytes(prec)
+    Cn = AB.copy()
+    for off in (0, es):
+        Cn[:, off:off + 4] = (-Cn[:, off:off + 4].copy().view(np.int32)).view(np.uint8)
+    for name, C in (("spread", Cc), ("cancel", Cn)):
+        mpb.fma(prec, M, a, b, dvec(prec, C, True), r, cplx=True)
+        bad, first = orc.mismatches(prec, hvec(prec, r, M, True), orc.fma(prec, A, B, C, "mp", cplx=True), True)
+        assert bad == 0, f"cfma {name} PB={prec}: {bad} mismatches, first at {first}"
+
+
 @pytest.mark.parametrize("cplx", (False, True))
 @pytest.mark.parametrize("prec", PRECS)
 @pytest.mark.parametrize("n", (1, 31, 33, 1000))

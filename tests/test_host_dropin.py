@@ -46,6 +46,54 @@ def test_complex_ops(orc, mpb, prec):
         assert bad == 0, f"{kind} PB={prec}: first mismatch {first}"
 
 
+def _negate_complex(orc, prec, Z):
+    """-Z for complex AoS elements (flip both components' sign words)."""
+    es = orc.elem_bytes(prec)
+    out = Z.copy()
+    for off in (0, es):
+        sgn = out[:, off:off + 4].copy().view(np.int32)
+        out[:, off:off + 4] = (-sgn).view(np.uint8)
+    return out
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_cfma_single_rounding(orc, mpb, prec):
+    """cu_cfma: a*b + c with one rounding per component, against the system
+    mpc_fma and, independently, mpc_dot over ([a, c], [b, 1]).  Cases: the
+    reference generator's wide exponent spreads (terms far apart: the
+    round-to-odd branch), c = -round(a*b) (cancellation down to the rounding
+    error of the product: the exact branch), a = (x, x) and b = (y, y)
+    (the two products cancel exactly in the real part), and zeros."""
+    H = mpb.host_lib()
+    M = 2000 if prec <= 1056 else 500
+    A, B = orc.gen_pairs(prec, M, 0x2222 + prec, cplx=True)
+    Cc, _ = orc.gen_pairs(prec, M, 0x3333 + prec, cplx=True)
+    es = orc.elem_bytes(prec)
+    # near-cancelling addend: -round(a*b)
+    AB = orc.empty(prec, M, True)
+    assert H.mpbh_cbinop(prec, 0, M, _p(A), _p(B), _p(AB)) == 0
+    Cn = _negate_complex(orc, prec, AB)
+    # a = (x, x), b = (y, y): re = x*y - x*y = 0 exactly, so re = round(c.re)
+    Ax, By = A.copy(), B.copy()
+    Ax[:, es:] = Ax[:, :es]
+    By[:, es:] = By[:, :es]
+    # zeros: every third a, b or c is 0 + 0i
+    zero = orc.binop("csub", prec, A[:1], A[:1], "mp")
+    Az, Bz, Cz = A.copy(), B.copy(), Cc.copy()
+    Az[0::3] = zero
+    Bz[1::3] = zero
+    Cz[2::3] = zero
+    for name, (a, b, c) in {"spread": (A, B, Cc), "cancel": (A, B, Cn), "products cancel": (Ax, By, Cc),
+                            "zeros": (Az, Bz, Cz)}.items():
+        R = orc.empty(prec, M, True)
+        assert H.mpbh_cfma(prec, M, _p(a), _p(b), _p(c), _p(R)) == 0
+        want = orc.fma(prec, a, b, c, impl="mp", cplx=True)
+        want2 = orc.fma(prec, a, b, c, impl="mpdot", cplx=True)
+        assert orc.mismatches(prec, want, want2, True)[0] == 0, f"{name}: mpc_fma and mpc_dot disagree"
+        bad, first = orc.mismatches(prec, R, want, True)
+        assert bad == 0, f"cfma {name} PB={prec}: {bad} mismatches, first at {first}"
+
+
 @pytest.mark.parametrize("cplx", (False, True))
 @pytest.mark.parametrize("prec", (64, 256, 1024))
 def test_axpy_host(orc, mpb, prec, cplx):
