@@ -42,7 +42,8 @@ struct Plan {
   int d0;              /* lowest diagonal of the main pass (0: all diagonals, no certification) */
   long cert;           /* log2 of the bound on the omitted diagonals' sum (LSB units); -1 when d0 = 0 */
   long units;          /* units of the main pass, diagonals [d0, 2S-2] */
-  size_t off_rowE, off_colE, off_flags, off_cnt, off_ef, off_tf, off_tiles, off_asl, off_bsl, off_d, total;
+  size_t off_rowE, off_colE, off_colEmin, off_flags, off_cnt, off_ef, off_tf, off_tiles, off_asl, off_bsl, off_d,
+      total;
 };
 
 static inline int ceil_log2(long x) {
@@ -105,6 +106,8 @@ static bool make_plan(int prec, size_t m, size_t n, size_t k, int sp_bits, int c
   o = up256(o + 4 * m);
   p.off_colE = o;
   o = up256(o + 4 * n);
+  p.off_colEmin = o;
+  o = up256(o + 4 * n);
   p.off_flags = o; /* m row flags then n column flags, one byte each */
   o = up256(o + m + n);
   p.off_cnt = o; /* [0] fallback rows+cols, [1] kernel error, [2] tiles to recompute */
@@ -144,12 +147,66 @@ __device__ __forceinline__ uint32_t head_of(const uint8_t *base, size_t idx, int
 /* ------------------------------------------------------------------ *
  * 1. exponent statistics
  * ------------------------------------------------------------------ */
+/* Column statistics of B first: k is split into chunks of kColRows rows, one
+ * block per (32 columns, chunk), and each block folds its partial max / min
+ * exponent into colE / colEmin with atomics (initialised to kColNone /
+ * kColMinNone by a byte memset).  k_row_stats then finalises the columns. */
+constexpr int kColRows = 128;
+constexpr int32_t kColNone = (int32_t)0x80808080;    /* memset 0x80: no nonzero entry seen */
+constexpr int32_t kColMinNone = (int32_t)0x7f7f7f7f; /* memset 0x7f */
+template <int N, bool CPLX>
+__global__ void __launch_bounds__(256) k_col_stats(int n, int k, const uint8_t *B, size_t ldb, int32_t *colE,
+                                                   int32_t *colEmin) {
+  __shared__ int32_t smax[8][32], smin[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int j = blockIdx.x * 32 + lane;
+  const int k0 = blockIdx.y * kColRows, k1 = min(k, k0 + kColRows);
+  int32_t emax = kColNone, emin = kColMinNone;
+  if (j < n) {
+    for (int kk = k0 + w; kk < k1; kk += 8) {
+#pragma unroll
+      for (int part = 0; part < (CPLX ? 2 : 1); ++part) {
+        const uint32_t h = head_of<N, CPLX>(B, (size_t)kk * ldb + j, part);
+        if (h != kHeadZero) {
+          const int32_t e = head_exp(h);
+          emax = max(emax, e);
+          emin = min(emin, e);
+        }
+      }
+    }
+  }
+  smax[w][lane] = emax;
+  smin[w][lane] = emin;
+  __syncthreads();
+  if (w == 0 && j < n) {
+    for (int q = 1; q < 8; ++q) {
+      emax = max(emax, smax[q][lane]);
+      emin = min(emin, smin[q][lane]);
+    }
+    if (emax != kColNone) {
+      atomicMax(colE + j, emax);
+      atomicMin(colEmin + j, emin);
+    }
+  }
+}
+
 /* one warp per row of A: E_i = max exponent of the nonzero entries (both
  * parts of a complex entry); flag the row when some nonzero entry lies more
- * than SP bits below E_i */
+ * than SP bits below E_i.  The same launch finalises the column statistics:
+ * an all-zero column gets kExpZero, a column whose spread exceeds SP is
+ * flagged; flagged rows and columns are counted. */
 template <int N, bool CPLX>
 __global__ void __launch_bounds__(256) k_row_stats(int m, int k, const uint8_t *A, size_t lda, int SP, int32_t *rowE,
-                                                   uint8_t *rowF, int *count) {
+                                                   uint8_t *rowF, int n, int32_t *colE, const int32_t *colEmin,
+                                                   uint8_t *colF, int *count) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int32_t e = colE[j];
+    const bool none = e == kColNone;
+    const bool flag = !none && (long)e - colEmin[j] > SP;
+    colE[j] = none ? kExpZero : e;
+    colF[j] = flag ? 1 : 0;
+    if (flag) atomicAdd(count, 1);
+  }
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= m) return;
   int32_t emax = kExpZero, emin = 0x7fffffff;
@@ -177,41 +234,6 @@ __global__ void __launch_bounds__(256) k_row_stats(int m, int k, const uint8_t *
     const bool flag = emax != kExpZero && (long)emax - emin > SP;
     rowF[warp] = flag ? 1 : 0;
     if (flag) atomicAdd(count, 1);
-  }
-}
-/* column statistics of B (k x n): block = 32 columns x 8 row groups */
-template <int N, bool CPLX>
-__global__ void __launch_bounds__(256) k_col_stats(int n, int k, const uint8_t *B, size_t ldb, int SP, int32_t *colE,
-                                                   uint8_t *colF, int *count) {
-  __shared__ int32_t smax[8][32], smin[8][32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int j = blockIdx.x * 32 + lane;
-  int32_t emax = kExpZero, emin = 0x7fffffff;
-  for (int kk = w; kk < k; kk += 8) {
-#pragma unroll
-    for (int part = 0; part < (CPLX ? 2 : 1); ++part) {
-      const uint32_t h = head_of<N, CPLX>(B, (size_t)kk * ldb + j, part);
-      if (h != kHeadZero) {
-        const int32_t e = head_exp(h);
-        emax = max(emax, e);
-        emin = min(emin, e);
-      }
-    }
-  }
-  smax[w][lane] = emax;
-  smin[w][lane] = emin;
-  __syncthreads();
-  if (w == 0) {
-    for (int q = 1; q < 8; ++q) {
-      emax = max(emax, smax[q][lane]);
-      emin = min(emin, smin[q][lane]);
-    }
-    if (j < n) {
-      colE[j] = emax;
-      const bool flag = emax != kExpZero && (long)emax - emin > SP;
-      colF[j] = flag ? 1 : 0;
-      if (flag) atomicAdd(count, 1);
-    }
   }
 }
 
@@ -251,19 +273,23 @@ __device__ __forceinline__ void aligned_twos(uint32_t (&w)[N + XL + 1], const fv
     }
   }
 }
-/* balanced base-256 digits of a two's complement integer: byte b plus the
- * incoming carry t becomes t - 256 (carry 1) when t >= 128.  For
- * |V| < 2^(8S-2) every digit above S-1 is zero, so put(s, d) is called for
- * s < S only. */
+/* balanced base-256 digits of a two's complement integer V: the digits in
+ * [-128, 127] with V = sum d_s 256^s are the bytes of U = V + 0x8080...80,
+ * each XOR 0x80 (adding 128 to every byte produces exactly the carries of
+ * the digit-by-digit recoding: byte b plus carry becomes b - 256, carry 1,
+ * when it reaches 128).  One carry chain for U, then every digit is a byte
+ * extraction.  For |V| < 2^(8S-2) every digit above S-1 is zero, so put(s, d)
+ * is called for s < S only. */
 template <int L1, typename F>
 __device__ __forceinline__ void twos_digits(const uint32_t (&w)[L1], int S, F put) {
-  uint32_t carry = 0;
+  uint32_t u[L1];
+  uint32_t cf = 0;
+  u[0] = add_cc(w[0], 0x80808080u, cf);
 #pragma unroll
-  for (int s = 0; s < 4 * L1; ++s) {
-    const uint32_t t = ((w[s >> 2] >> (8 * (s & 3))) & 0xffu) + carry;
-    carry = (t >= 128u) ? 1u : 0u;
-    if (s < S) put(s, (int8_t)(carry ? (int)t - 256 : (int)t));
-  }
+  for (int i = 1; i < L1; ++i) u[i] = addc_cc(w[i], 0x80808080u, cf);
+#pragma unroll
+  for (int s = 0; s < 4 * L1; ++s)
+    if (s < S) put(s, (int8_t)(((u[s >> 2] >> (8 * (s & 3))) & 0xffu) ^ 0x80u));
 }
 /* the digit stream of one element for product q: 0 (real / re part),
  * 1 (im), 2 (re + im) */
@@ -310,51 +336,30 @@ __global__ void __launch_bounds__(128) k_slice_a(int m, int k, int kp, const uin
   }
 }
 
-/* B (k x n, tiles) -> B_sl[q*S+s][j][kp], transposed through shared memory:
- * block = 32 columns (one tile) x 32 rows of B; digits staged per 32-plane
- * chunk as [s][j][32 bytes of k], written out as 32-byte row segments. */
+/* B (k x n, tiles) -> B_sl[q*S+s][j][kp]: thread per (j, kk) with kk running
+ * fastest across the lanes, so each digit plane is written as 32-byte rows
+ * (one byte per lane) and no staging is needed; the lanes' element loads
+ * come from 32 rows of B (16-byte pieces whose tile neighbours are read by
+ * the warps of columns j +- 1 soon after, from L2). */
 template <int N, int XL, bool CPLX>
-__global__ void __launch_bounds__(256) k_slice_b(int n, int k, int kp, const uint8_t *B, size_t ldb, int SP, int S,
+__global__ void __launch_bounds__(128) k_slice_b(int n, int k, int kp, const uint8_t *B, size_t ldb, int SP, int S,
                                                  const int32_t *colE, const uint8_t *colF, int8_t *Bsl) {
-  constexpr int CH = 32; /* digit planes per chunk */
-  __shared__ __align__(16) int8_t st[CH][32][32 + 16];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
-  const int j = j0 + lane;
-  const size_t plane = (size_t)n * kp;
-  fval<N> xr[4], xi[4];
-  const int32_t E = (j < n) ? colE[j] : kExpZero;
-  const bool skip = (j >= n) || colF[j];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const int kk = k0 + w + 8 * r;
-    set_zero(xi[r]);
-    if (kk < k && !skip)
-      load_any<N, CPLX>(xr[r], xi[r], B, (size_t)kk * ldb + j);
+  const size_t total = (size_t)n * kp, plane = (size_t)n * kp;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(idx / kp), kk = (int)(idx % kp);
+    fval<N> re, im;
+    set_zero(im);
+    if (kk < k && !colF[j])
+      load_any<N, CPLX>(re, im, B, (size_t)kk * ldb + j);
     else
-      set_zero(xr[r]);
-  }
+      set_zero(re);
+    const int32_t E = colE[j];
+    int8_t *dst = Bsl + (size_t)j * kp + kk;
 #pragma unroll 1
-  for (int q = 0; q < (CPLX ? 3 : 1); ++q) {
-    for (int c0 = 0; c0 < S; c0 += CH) {
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int kl = w + 8 * r;
-        element_digits<N, XL, CPLX>(xr[r], xi[r], E, SP, S, q, [&](int s, int8_t d) {
-          if (s >= c0 && s < c0 + CH) st[s - c0][lane][kl] = d;
-        });
-      }
-      __syncthreads();
-      /* write: for each plane s and column jl, 32 bytes of k (two uint4) */
-      const int nplanes = min(CH, S - c0);
-      for (int t = threadIdx.x; t < nplanes * 32 * 2; t += blockDim.x) {
-        const int half = t & 1, jl = (t >> 1) & 31, s = t >> 6;
-        if (j0 + jl < n) {
-          const uint4 v = *(const uint4 *)&st[s][jl][16 * half];
-          *(uint4 *)(Bsl + (size_t)(q * S + c0 + s) * plane + (size_t)(j0 + jl) * kp + k0 + 16 * half) = v;
-        }
-      }
-      __syncthreads();
+    for (int q = 0; q < (CPLX ? 3 : 1); ++q) {
+      int8_t *dq = dst + (size_t)q * S * plane;
+      element_digits<N, XL, CPLX>(re, im, E, SP, S, q, [&](int s, int8_t d) { dq[(size_t)s * plane] = d; });
     }
   }
 }
@@ -388,6 +393,19 @@ template <int N, int XL>
 struct round_geo {
   static constexpr int SMAX = 4 * (N + XL);
   static constexpr int Q = (8 * (2 * SMAX - 2) + 31 + 8 + 31) / 32 + 1;
+  /* the single-part first pass reads at most J planes, from d0 on; their sum
+   * (coefficients up to 3) spans 8(J-1) + 35 bits with the sign */
+  static constexpr int J = SMAX + 20;
+  static constexpr int QJ = (8 * (J - 1) + 35 + 31) / 32 + 1;
+  /* threads per block of the first pass: each keeps (QJ | 1) words per
+   * component in shared memory, within the 48 KB static limit.  The launch
+   * bound asks for 5 (10) resident blocks, i.e. at most ~100 registers: the
+   * pass is latency-bound and needs many warps, each with a batch of plane
+   * loads in flight, more than registers per thread. */
+  template <bool CPLX>
+  static constexpr int threads() {
+    return 128 * (QJ | 1) * (CPLX ? 2 : 1) * 4 <= 46 * 1024 ? 128 : 64;
+  }
 };
 
 /* Normalise and round once: v[0..W) is the two's complement integer
@@ -462,6 +480,57 @@ __device__ __forceinline__ bool round_words(fval<N> &r, uint32_t (&v)[W], long l
   return ok;
 }
 
+/* round_words for a sum held in shared memory (this thread's W words at
+ * sv[0..W), stride 1): the words are negated in place when negative, then only
+ * the N + 2 words under the leading bit are read (runtime index from the top
+ * word) and the rest is OR-ed into the sticky bit, so no register array of W
+ * words and no shift network over it is needed.  Same result and the same
+ * certification as round_words. */
+template <int N, int W>
+__device__ __forceinline__ bool round_smem(fval<N> &r, uint32_t *sv, long lsb_exp, long cert) {
+  static_assert(W >= N + 2, "word window too small");
+  const uint32_t neg = sv[W - 1] >> 31;
+  if (neg) {
+    uint32_t c = 1;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      const uint32_t t = ~sv[w] + c;
+      c = (c && t == 0) ? 1u : 0u;
+      sv[w] = t;
+    }
+  }
+  int top = -1;
+#pragma unroll
+  for (int w = 0; w < W; ++w) top = sv[w] != 0u ? w : top;
+  if (top < 0) {
+    set_zero(r);
+    return cert < 0;
+  }
+  auto word = [&](int i) -> uint32_t { return i >= 0 ? sv[i] : 0u; };
+  const uint32_t lr = clz32(sv[top]) & 31u;
+#pragma unroll
+  for (int i = 0; i < N; ++i) r.m[N - 1 - i] = fshl(word(top - i - 1), word(top - i), lr);
+  const uint32_t g = fshl(word(top - N - 1), word(top - N), lr);
+  const uint32_t nx = fshl(word(top - N - 2), word(top - N - 1), lr);
+  uint32_t st = (g << 1) | (word(top - N - 1) << lr);
+#pragma unroll
+  for (int w = 0; w < W; ++w) st |= (w <= top - N - 2) ? sv[w] : 0u;
+  const long msb = 32L * top + 31 - lr;
+  bool ok = true;
+  if (cert >= 0) {
+    const long t = cert - (msb - 32L * N + 1); /* log2 of the bound in ULPs */
+    const uint64_t G = ((uint64_t)g << 32) | nx;
+    const uint64_t thr = (t < -64) ? 1ull : (1ull << (64 + t));
+    const uint64_t half = 1ull << 63;
+    ok = t <= -3 && (G <= half - thr - 1 || G > half + thr);
+  }
+  int32_t ee = (int32_t)(msb + 1 + lsb_exp);
+  rndn<N>(r.m, ee, g >> 31, st);
+  r.e = ee;
+  r.s = neg;
+  return ok;
+}
+
 /* One rounding pass of the exact GEMM (both kernels below).
  * Pass 1 (flagged_only = 0) visits every entry, sums the diagonals
  * [d_first, 2S-2] and, when d_first > 0, certifies the rounding against the
@@ -505,20 +574,31 @@ __device__ __forceinline__ void mark_tile(const RoundPass &rp, int i, int j) {
   if (atomicExch(rp.tf + tile, 1) == 0) rp.tiles[atomicAdd(rp.ntiles, 1)] = tile;
 }
 
-/* Single k-part (P == 1): the diagonal planes of output idx are streamed
- * word by word -- word w gathers diagonals 4w..4w+3 (each < 2^31, times
- * 2^(8j) < 2^24) plus the carry of word w-1, keeps its low 32 bits and
- * carries the rest on, so no wide accumulator is held.  Complex outputs read
- * each product's plane once and form both components: re = T0 - T1,
- * im = T2 - T0 - T1.  Every loop is unrolled at compile time. */
+/* First pass with a single k-part (P == 1) and at most J planes from
+ * d_first on: the planes of output idx are loaded BATCH at a time (many
+ * independent loads in flight per thread) and streamed into 32-bit words
+ * with an int64 carry -- plane d_first + j lands in word j/4, byte j%4.  The words hold the sum divided by 256^d_first, so the
+ * LSB exponent and the certification bound move up by 8 d_first bits instead
+ * of the words moving.  Complex outputs read each product's planes once and
+ * form both components: re = T0 - T1, im = T2 - T0 - T1.  Every loop is
+ * unrolled at compile time. */
 template <int N, int XL, bool CPLX>
-__global__ void __launch_bounds__(128) k_exact_round(int m, int n, int S, int SP, const int32_t *D,
-                                                     const int32_t *rowE, const int32_t *colE, const uint8_t *rowF,
-                                                     const uint8_t *colF, uint8_t *C, size_t ldc, RoundPass rp) {
-  constexpr int Q = round_geo<N, XL>::Q;
-  constexpr int DMAX = 2 * round_geo<N, XL>::SMAX - 1;
+__global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
+                                  round_geo<N, XL>::template threads<CPLX>() == 128 ? 5 : 10)
+    k_exact_round(int m, int n, int S, int SP, const int32_t *D, const int32_t *rowE, const int32_t *colE,
+                  const uint8_t *rowF, const uint8_t *colF, uint8_t *C, size_t ldc, RoundPass rp) {
+  constexpr int J = round_geo<N, XL>::J;
+  constexpr int QJ = round_geo<N, XL>::QJ;
+  constexpr int SW = QJ | 1; /* odd word stride per thread: conflict-free banks */
+  constexpr int T = round_geo<N, XL>::template threads<CPLX>();
+  __shared__ uint32_t swords[T * SW * (CPLX ? 2 : 1)];
+  uint32_t *svr = swords + threadIdx.x * SW * (CPLX ? 2 : 1);
+  uint32_t *svi = svr + SW;
+  constexpr int BATCH = 16; /* a multiple of 4 */
+  static_assert(4 * QJ >= J, "words must cover the planes");
   const size_t total = pass_total(rp, m, n), plane = (size_t)m * n;
   const int ndiag = 2 * S - 1;
+  const int nl = ndiag - rp.d_first; /* <= J, checked on the host */
   const size_t qstride = (size_t)ndiag * plane;
   for (size_t u = (size_t)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (size_t)gridDim.x * blockDim.x) {
     int i, j;
@@ -528,42 +608,59 @@ __global__ void __launch_bounds__(128) k_exact_round(int m, int n, int S, int SP
       if (!rp.flagged_only) rp.ef[idx] = 0;
       continue;
     }
-    const long lsb = (long)rowE[i] + colE[j] - 2L * (32 * N) - 2L * SP;
-    uint32_t vr[Q], vi[CPLX ? Q : 1];
+    /* BATCH planes of every product in flight, then their BATCH/4 words
+     * (kept in this thread's shared-memory slot):
+     * word w = carry + sum of planes 4w..4w+3 (each < 2^31, times 2^(8j)),
+     * low 32 bits kept, the rest carried on */
     long long cr = 0, ci = 0;
-    const int32_t *d0 = D + idx;
+    const int32_t *base = D + (size_t)rp.d_first * plane + idx;
 #pragma unroll
-    for (int w = 0; w < Q; ++w) {
-      long long tr = cr, ti = ci;
+    for (int j0 = 0; j0 < 4 * QJ; j0 += BATCH) {
+      int32_t t0v[BATCH], t1v[CPLX ? BATCH : 1], t2v[CPLX ? BATCH : 1];
 #pragma unroll
-      for (int jj = 0; jj < 4; ++jj) {
-        const int d = 4 * w + jj;
-        if (d < DMAX && d < ndiag && d >= rp.d_first) {
-          const long long scale = 1LL << (8 * jj);
-          const long long t0 = __ldcs(d0 + (size_t)d * plane);
+      for (int jj = 0; jj < BATCH; ++jj) {
+        const bool in = j0 + jj < nl;
+        const size_t off = (size_t)(j0 + jj) * plane;
+        t0v[jj] = in ? __ldcs(base + off) : 0;
+        if (CPLX) {
+          t1v[jj] = in ? __ldcs(base + qstride + off) : 0;
+          t2v[jj] = in ? __ldcs(base + 2 * qstride + off) : 0;
+        }
+      }
+#pragma unroll
+      for (int w4 = 0; w4 < BATCH / 4; ++w4) {
+        const int w = j0 / 4 + w4;
+        if (w < QJ) {
+          long long tr = cr, ti = ci;
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const long long scale = 1LL << (8 * jj);
+            const long long t0 = t0v[4 * w4 + jj];
+            if (CPLX) {
+              const long long t1 = t1v[4 * w4 + jj], t2 = t2v[4 * w4 + jj];
+              tr += (t0 - t1) * scale;
+              ti += (t2 - t0 - t1) * scale;
+            } else {
+              tr += t0 * scale;
+            }
+          }
+          svr[w] = (uint32_t)tr;
+          cr = tr >> 32;
           if (CPLX) {
-            const long long t1 = __ldcs(d0 + qstride + (size_t)d * plane);
-            const long long t2 = __ldcs(d0 + 2 * qstride + (size_t)d * plane);
-            tr += (t0 - t1) * scale;
-            ti += (t2 - t0 - t1) * scale;
-          } else {
-            tr += t0 * scale;
+            svi[w] = (uint32_t)ti;
+            ci = ti >> 32;
           }
         }
       }
-      vr[w] = (uint32_t)tr;
-      cr = tr >> 32;
-      if (CPLX) {
-        vi[w] = (uint32_t)ti;
-        ci = ti >> 32;
-      }
     }
+    const long lsb = (long)rowE[i] + colE[j] - 2L * (32 * N) - 2L * SP + 8L * rp.d_first;
     /* an all-zero row or column has all-zero digits: its sum is exactly 0 */
-    const long cert = (rowE[i] == kExpZero || colE[j] == kExpZero) ? -1 : rp.cert;
+    const long cert =
+        (rowE[i] == kExpZero || colE[j] == kExpZero || rp.cert < 0) ? -1 : rp.cert - 8L * rp.d_first;
     fval<N> re;
-    bool ok = round_words<N, Q>(re, vr, lsb, cert);
+    bool ok = round_smem<N, QJ>(re, svr, lsb, cert);
     fval<N> im;
-    if (CPLX) ok = round_words<N, Q>(im, *reinterpret_cast<uint32_t(*)[Q]>(vi), lsb, cert) && ok;
+    if (CPLX) ok = round_smem<N, QJ>(im, svi, lsb, cert) && ok;
     if (!rp.flagged_only) {
       rp.ef[idx] = ok ? 0 : 1;
       if (!ok) {
@@ -704,9 +801,17 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
       cudaMemsetAsync(rp.tf, 0, 4 * (size_t)p.mt * p.nt, st) != cudaSuccess)
     return MPB_ERR_CUDA;
 
+  int32_t *colEmin = (int32_t *)(ws + p.off_colEmin);
+  if (cudaMemsetAsync(colE, 0x80, 4 * (size_t)p.n, st) != cudaSuccess ||
+      cudaMemsetAsync(colEmin, 0x7f, 4 * (size_t)p.n, st) != cudaSuccess)
+    return MPB_ERR_CUDA;
   profile_mark(kPhaseStats, true, st);
-  k_row_stats<N, CPLX><<<(p.m + 7) / 8, 256, 0, st>>>(p.m, p.k, A, lda, p.SP, rowE, rowF, cnt);
-  k_col_stats<N, CPLX><<<(p.n + 31) / 32, 256, 0, st>>>(p.n, p.k, B, ldb, p.SP, colE, colF, cnt);
+  {
+    const dim3 grid((p.n + 31) / 32, (p.k + kColRows - 1) / kColRows);
+    k_col_stats<N, CPLX><<<grid, 256, 0, st>>>(p.n, p.k, B, ldb, colE, colEmin);
+  }
+  k_row_stats<N, CPLX><<<(p.m + 7) / 8, 256, 0, st>>>(p.m, p.k, A, lda, p.SP, rowE, rowF, p.n, colE, colEmin, colF,
+                                                      cnt);
   profile_mark(kPhaseStats, false, st);
   profile_mark(kPhaseSlice, true, st);
   {
@@ -714,8 +819,8 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
     k_slice_a<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.k, p.kp, A, lda, p.SP, p.S, rowE, rowF, Asl);
   }
   {
-    const dim3 grid((p.n + 31) / 32, p.kp / 32);
-    k_slice_b<N, XL, CPLX><<<grid, 256, 0, st>>>(p.n, p.k, p.kp, B, ldb, p.SP, p.S, colE, colF, Bsl);
+    const int g = grid_for(k_slice_b<N, XL, CPLX>, 128, (size_t)p.n * p.kp);
+    k_slice_b<N, XL, CPLX><<<g, 128, 0, st>>>(p.n, p.k, p.kp, B, ldb, p.SP, p.S, colE, colF, Bsl);
   }
   profile_mark(kPhaseSlice, false, st);
   if (launch_status() != MPB_OK) return MPB_ERR_CUDA;
@@ -726,9 +831,10 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
     if (rc != MPB_OK) return rc;
   }
   auto round_pass = [&](const RoundPass &r, int grid_cap) {
-    if (p.P == 1) {
-      const int g = std::min(grid_cap, grid_for(k_exact_round<N, XL, CPLX>, 128, (size_t)p.m * p.n));
-      k_exact_round<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.n, p.S, p.SP, D, rowE, colE, rowF, colF, C, ldc, r);
+    if (p.P == 1 && !r.flagged_only && 2 * p.S - 1 - r.d_first <= round_geo<N, XL>::J) {
+      constexpr int T = round_geo<N, XL>::template threads<CPLX>();
+      const int g = std::min(grid_cap, grid_for(k_exact_round<N, XL, CPLX>, T, (size_t)p.m * p.n));
+      k_exact_round<N, XL, CPLX><<<g, T, 0, st>>>(p.m, p.n, p.S, p.SP, D, rowE, colE, rowF, colF, C, ldc, r);
     } else {
       const int g = std::min(grid_cap, grid_for(k_exact_round_parts<N, XL, CPLX>, 128, (size_t)p.m * p.n));
       k_exact_round_parts<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.n, p.S, p.SP, p.P, D, rowE, colE, rowF, colF, C,

@@ -206,6 +206,28 @@ def test_exact_complex_vs_mpc_dot(orc, mpb, prec, shape):
     assert bad == 0, f"PB={prec} {shape}: {bad} mismatches, first at {first}"
 
 
+@pytest.mark.parametrize("cplx", (False, True))
+@pytest.mark.parametrize("sp_bits", (16, 32, 100))
+@pytest.mark.parametrize("prec", (64, 128, 256, 512, 1024, 2048))
+def test_exact_every_slice_geometry(orc, mpb, prec, sp_bits, cplx):
+    """Every (precision, spread budget) instantiation of the slicing and
+    rounding kernels -- the budget picks 1, 2 or 4 extra words for the aligned
+    integers -- against mpfr_dot / mpc_dot, on a shape with a ragged last tile."""
+    if cplx and prec == 2048:
+        pytest.skip("complex PB=2048 is covered by the plain kernels")
+    m, n, k = 9, 37, 45
+    if cplx:
+        A, B = rand_caos(prec, m * k, 61 + sp_bits, -6, 6, 0.02), rand_caos(prec, k * n, 62 + sp_bits, -6, 6, 0.02)
+        C, st = run_exact_c(mpb, prec, m, n, k, A, B, sp_bits=sp_bits)
+    else:
+        A, B = rand_aos(prec, m * k, 61 + sp_bits, -6, 6, 0.02), rand_aos(prec, k * n, 62 + sp_bits, -6, 6, 0.02)
+        C, st = run_exact(mpb, prec, m, n, k, A, B, sp_bits=sp_bits)
+    assert st[1] == 0 and st[0] == 0
+    exp = orc.gemm_exact(prec, m, n, k, A, k, B, n, cplx=cplx, impl="mp")
+    bad, first = orc.mismatches(prec, C, exp, cplx)
+    assert bad == 0, f"PB={prec} sp={sp_bits} cplx={cplx}: {bad} mismatches, first at {first}"
+
+
 def test_exact_complex_fallback(orc, mpb):
     prec, m, n, k = 256, 12, 40, 30
     A = rand_caos(prec, m * k, 41, -4, 4, 0.0).reshape(m, k, -1)
