@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       const Unit x = decode(g, u, T);
       sm100::tc_fence_after();
       const int row = x.ti * BM + q * 32 + lane;
-      int32_t *drow = g.D + ((((size_t)x.q * g.P + x.part) * (2 * g.S - 1) + x.d) * g.m + (size_t)row) * g.n;
+      int32_t *drow = g.D + (((size_t)x.q * g.P + x.part) * (2 * g.S - 1) + x.d) * g.dplane + (size_t)row * g.n;
       const uint32_t tacc = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
 #pragma unroll 1
       for (int c = 0; c < BN / 32; ++c) {
@@ -328,6 +328,7 @@ int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *e
   ga.KC = p.KC;
   ga.m = p.m;
   ga.n = p.n;
+  ga.dplane = p.dplane;
   ga.dl = dl;
   ga.dh = dh;
   ga.units = (long)p.nprod * (dh - dl + 1) * p.mt * p.nt * p.P;

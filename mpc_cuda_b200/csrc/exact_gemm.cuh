@@ -40,6 +40,7 @@ struct Plan {
   int P, cpp;          /* k-parts per diagonal, chunks per part */
   int mt, nt;          /* tiles */
   int d0;              /* lowest diagonal of the main pass (0: all diagonals, no certification) */
+  size_t dplane;       /* elements from one diagonal plane to the next (m*n, padded) */
   long cert;           /* log2 of the bound on the omitted diagonals' sum (LSB units); -1 when d0 = 0 */
   long units;          /* units of the main pass, diagonals [d0, 2S-2] */
   size_t off_rowE, off_colE, off_colEmin, off_flags, off_cnt, off_ef, off_tf, off_tiles, off_asl, off_bsl, off_d,
@@ -101,6 +102,11 @@ static bool make_plan(int prec, size_t m, size_t n, size_t k, int sp_bits, int c
     }
   }
   p.units = (long)p.nprod * (2 * p.S - 1 - p.d0) * p.mt * p.nt * p.P;
+  /* Diagonal planes are m*n int32 each; the rounding reads one entry from
+   * every plane, so a power-of-two plane size would send all of those loads
+   * to the same DRAM channels.  The stride is padded by 4224 bytes (33 x 128)
+   * to spread them; it stays a multiple of 128 bytes. */
+  p.dplane = (m * n + 31) / 32 * 32 + 1056;
   size_t o = 0;
   p.off_rowE = o;
   o = up256(o + 4 * m);
@@ -123,7 +129,7 @@ static bool make_plan(int prec, size_t m, size_t n, size_t k, int sp_bits, int c
   p.off_bsl = o;
   o = up256(o + (size_t)p.nprod * p.S * n * p.kp);
   p.off_d = o;
-  o = up256(o + (size_t)p.nprod * p.P * (2 * p.S - 1) * m * n * 4);
+  o = up256(o + (size_t)p.nprod * p.P * (2 * p.S - 1) * p.dplane * 4);
   p.total = o;
   return true;
 }
@@ -369,11 +375,12 @@ __global__ void __launch_bounds__(128) k_slice_b(int n, int k, int kp, const uin
  * ------------------------------------------------------------------ */
 struct GemmArgs {
   int S, nprod, mt, nt, P, cpp, KC, m, n;
+  size_t dplane;       /* elements between consecutive diagonal planes */
   int dl, dh;          /* diagonals computed: [dl, dh] */
   long units;          /* all tiles (tiles == nullptr) */
   const int *tiles;    /* or only these output tiles ... */
   const int *ntiles;   /* ... *ntiles of them, counted on the device */
-  int32_t *D;          /* [nprod][P][2S-1][m][n] */
+  int32_t *D;          /* [nprod][P][2S-1][dplane], each plane m x n */
   int *err;
 };
 
@@ -540,6 +547,7 @@ __device__ __forceinline__ bool round_smem(fval<N> &r, uint32_t *sv, long lsb_ex
  * set, after the tensor cores have filled in their low diagonals, and rounds
  * the full sum (d_first = 0, no certification). */
 struct RoundPass {
+  size_t dplane; /* elements between consecutive diagonal planes */
   int d_first;
   long cert;
   int flagged_only;
@@ -575,17 +583,18 @@ __device__ __forceinline__ void mark_tile(const RoundPass &rp, int i, int j) {
 }
 
 /* First pass with a single k-part (P == 1) and at most J planes from
- * d_first on: the planes of output idx are loaded BATCH at a time (many
- * independent loads in flight per thread) and streamed into 32-bit words
- * with an int64 carry -- plane d_first + j lands in word j/4, byte j%4.  The words hold the sum divided by 256^d_first, so the
- * LSB exponent and the certification bound move up by 8 d_first bits instead
- * of the words moving.  Complex outputs read each product's planes once and
- * form both components: re = T0 - T1, im = T2 - T0 - T1.  Every loop is
- * unrolled at compile time. */
+ * d_first on: the planes of output idx are loaded BATCH at a time and
+ * streamed into 32-bit words with an int64 carry -- plane d_first + j lands
+ * in word j/4, byte j%4.  The words hold the sum divided by 256^d_first, so
+ * the LSB exponent and the certification bound move up by 8 d_first bits
+ * instead of the words moving.  The words then go to the thread's slot in
+ * shared memory, where round_smem reads only the ones it needs.  Complex
+ * outputs read each product's planes once and form both components:
+ * re = T0 - T1, im = T2 - T0 - T1.  Every loop is unrolled at compile time. */
 template <int N, int XL, bool CPLX>
 __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
                                   round_geo<N, XL>::template threads<CPLX>() == 128 ? 5 : 10)
-    k_exact_round(int m, int n, int S, int SP, const int32_t *D, const int32_t *rowE, const int32_t *colE,
+    k_exact_round(int m, int n, int S, int SP, const int32_t *__restrict__ D, const int32_t *rowE, const int32_t *colE,
                   const uint8_t *rowF, const uint8_t *colF, uint8_t *C, size_t ldc, RoundPass rp) {
   constexpr int J = round_geo<N, XL>::J;
   constexpr int QJ = round_geo<N, XL>::QJ;
@@ -594,9 +603,9 @@ __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
   __shared__ uint32_t swords[T * SW * (CPLX ? 2 : 1)];
   uint32_t *svr = swords + threadIdx.x * SW * (CPLX ? 2 : 1);
   uint32_t *svi = svr + SW;
-  constexpr int BATCH = 16; /* a multiple of 4 */
+  constexpr int BATCH = CPLX ? 8 : 16; /* a multiple of 4 */
   static_assert(4 * QJ >= J, "words must cover the planes");
-  const size_t total = pass_total(rp, m, n), plane = (size_t)m * n;
+  const size_t total = pass_total(rp, m, n), plane = rp.dplane;
   const int ndiag = 2 * S - 1;
   const int nl = ndiag - rp.d_first; /* <= J, checked on the host */
   const size_t qstride = (size_t)ndiag * plane;
@@ -608,10 +617,10 @@ __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
       if (!rp.flagged_only) rp.ef[idx] = 0;
       continue;
     }
-    /* BATCH planes of every product in flight, then their BATCH/4 words
-     * (kept in this thread's shared-memory slot):
+    /* BATCH planes of every product in flight, then their BATCH/4 words:
      * word w = carry + sum of planes 4w..4w+3 (each < 2^31, times 2^(8j)),
      * low 32 bits kept, the rest carried on */
+    uint32_t vr[QJ], vi[CPLX ? QJ : 1];
     long long cr = 0, ci = 0;
     const int32_t *base = D + (size_t)rp.d_first * plane + idx;
 #pragma unroll
@@ -644,14 +653,21 @@ __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
               tr += t0 * scale;
             }
           }
-          svr[w] = (uint32_t)tr;
+          vr[w] = (uint32_t)tr;
           cr = tr >> 32;
           if (CPLX) {
-            svi[w] = (uint32_t)ti;
+            vi[w] = (uint32_t)ti;
             ci = ti >> 32;
           }
         }
       }
+    }
+    /* words to this thread's shared-memory slot only now, so that no store
+     * separates the batches of plane loads above */
+#pragma unroll
+    for (int w = 0; w < QJ; ++w) {
+      svr[w] = vr[w];
+      if (CPLX) svi[w] = vi[w];
     }
     const long lsb = (long)rowE[i] + colE[j] - 2L * (32 * N) - 2L * SP + 8L * rp.d_first;
     /* an all-zero row or column has all-zero digits: its sum is exactly 0 */
@@ -684,7 +700,7 @@ __global__ void __launch_bounds__(128) k_exact_round_parts(int m, int n, int S, 
                                                            const uint8_t *rowF, const uint8_t *colF, uint8_t *C,
                                                            size_t ldc, RoundPass rp) {
   constexpr int Q = round_geo<N, XL>::Q;
-  const size_t total = pass_total(rp, m, n), plane = (size_t)m * n;
+  const size_t total = pass_total(rp, m, n), plane = rp.dplane;
   const int ndiag = 2 * S - 1;
   const size_t pstride = (size_t)ndiag * plane, qstride = (size_t)P * pstride;
   for (size_t u = (size_t)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (size_t)gridDim.x * blockDim.x) {
@@ -789,6 +805,7 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
   int8_t *Asl = (int8_t *)(ws + p.off_asl), *Bsl = (int8_t *)(ws + p.off_bsl);
   int32_t *D = (int32_t *)(ws + p.off_d);
   RoundPass rp;
+  rp.dplane = p.dplane;
   rp.d_first = p.d0;
   rp.cert = p.cert;
   rp.flagged_only = 0;

@@ -71,11 +71,11 @@ def test_empty_inputs_are_noops(mpb):
 
 def test_exact_gemm_workspace_and_checks(mpb):
     L = mpb.lib()
-    # PB=512, 1024^3, 32-bit spread: S = 69 digit planes, 137 diagonals, plus
-    # one certification flag byte per entry
+    # PB=512, 1024^3, 32-bit spread: S = 69 digit planes, 137 diagonals (each
+    # padded by 1056 entries), plus one certification flag byte per entry
     S, m = 69, 1024
     need = L.mpb_gemm_exact_workspace(512, m, m, m, 32)
-    planes = S * 2 * m * m + 137 * m * m * 4 + m * m
+    planes = S * 2 * m * m + 137 * (m * m + 1056) * 4 + m * m
     assert planes <= need <= planes + 64 * 1024
     # the tensor cores skip the low diagonals 0..62: 2745 of the 69^2 slice pairs
     assert mpb.gemm_exact_info(512, m, m, m, 32) == (69, 63, 2745)
@@ -94,7 +94,7 @@ def test_exact_gemm_complex_workspace(mpb):
     # PB=256, 512^3 complex, 16-bit spread: S = ceil((256+16+3)/8) = 35, 3 products
     S, m = 35, 512
     need = L.mpb_gemm_exact_c_workspace(256, m, m, m, 16)
-    planes = 3 * S * 2 * m * m + 3 * (2 * S - 1) * m * m * 4 + m * m
+    planes = 3 * S * 2 * m * m + 3 * (2 * S - 1) * (m * m + 1056) * 4 + m * m
     assert planes <= need <= planes + 64 * 1024
     assert L.mpb_gemm_exact_c(256, 8, 8, 8, 4096, 32, 4096, 32, 4096, 32, 16, None, 0, None, None) == -8
 
