@@ -135,6 +135,15 @@ def imad_peak(stream_ptr):
     return v if v > 0 else None
 
 
+def rounded_product_imads(N):
+    """32-bit multiply-adds (lo + hi per limb pair) of one correctly rounded
+    N-limb product as the engine computes it: from N = 4 up only the columns
+    N-2 .. 2N-2 of the limb product (the rare full-product case aside)."""
+    if N < 4:
+        return 2 * N * N
+    return 2 * ((N - 1) + N + N * (N - 1) // 2)
+
+
 # ------------------------------------------------------------------ workloads
 class AxpyWorkload:
     """z = a*x + y over n elements (real or complex), rotating input sets so
@@ -219,7 +228,8 @@ class AxpyWorkload:
 
     def roofline(self, kernel_s, peaks, imad_ops_s):
         N = self.prec // 32
-        imad_per_unit = self.products * 2 * N * N  # schoolbook lo+hi multiply-adds
+        # complex: 4 exact (full) products; real: one rounded (upper-column) product
+        imad_per_unit = 4 * 2 * N * N if self.cplx else rounded_product_imads(N)
         bytes_per_unit = 3 * self.elem_bytes
         imad = imad_per_unit * self.n / kernel_s
         gbs = bytes_per_unit * self.n / kernel_s / 1e9
@@ -526,7 +536,7 @@ class GemvBatchWorkload:
             p, m, n = pr["prec"], pr["m"], pr["n"]
             N, eb = p // 32, 4 * (p // 32 + 1)
             u, o, b = out.get(p, (0, 0, 0))
-            out[p] = (u + m * n, o + 2 * N * N * m * n, b + (m * n + n + 2 * m) * eb)
+            out[p] = (u + m * n, o + rounded_product_imads(N) * m * n, b + (m * n + n + 2 * m) * eb)
         return out
 
     def roofline(self, kernel_s, peaks, imad_ops_s):

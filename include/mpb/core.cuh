@@ -11,7 +11,7 @@
  *
  * Every operation is round-to-nearest-even (MPFR_RNDN) with one rounding per
  * operation:
- *   mul          round(a*b)                (full N x N -> 2N product)
+ *   mul          round(a*b)                (upper half of the N x N product, certified)
  *   add_round    round(x + y)              (x, y exact NX-limb terms, result NM limbs)
  *   fma          round(a*b + c)            (single rounding)
  *   fmms/fmma    round(a*b -/+ c*d)        (single rounding; complex multiply)
@@ -48,8 +48,10 @@
 
 #if defined(__CUDACC__)
 #define MPB_UNROLL _Pragma("unroll")
+#define MPB_NOINLINE __host__ __device__ __noinline__
 #else
 #define MPB_UNROLL
+#define MPB_NOINLINE
 #endif
 
 namespace mpb {
@@ -257,11 +259,64 @@ MPB_HD bool is_zero(const fval<N> &x) {
   return x.e == kExpZero;
 }
 
+/* the upper columns only: p[N-2 .. 2N-1] of T = sum_{i+j >= N-2} a_i b_j
+ * 2^(32(i+j)), in the same product-scanning order as mul_full; the omitted
+ * pairs sum to L < (N-2) 2^(32(N-1)), below 2^38 units of word N-2 (N <= 64) */
 template <int N>
-MPB_HD void mul(fval<N> &r, const fval<N> &a, const fval<N> &b) {
+MPB_HD void mul_high(uint32_t *p, const uint32_t *a, const uint32_t *b) {
+  uint32_t c0 = 0u, c1 = 0u, c2 = 0u;
+  MPB_UNROLL
+  for (int c = N - 2; c < 2 * N - 1; ++c) {
+    MPB_UNROLL
+    for (int i = 0; i < N; ++i) {
+      const int j = c - i;
+      if (j < 0 || j >= N) continue;
+      uint32_t cf = 0;
+      c0 = madlo_cc(a[i], b[j], c0, cf);
+      c1 = madchi_cc(a[i], b[j], c1, cf);
+      c2 = addc(c2, 0u, cf);
+    }
+    p[c] = c0;
+    c0 = c1;
+    c1 = c2;
+    c2 = 0u;
+  }
+  p[2 * N - 1] = c0;
+}
+
+/* the full product and its rounding, out of line: the rare case of mul */
+template <int N>
+MPB_NOINLINE void mul_full_round(fval<N> &r, const fval<N> &a, const fval<N> &b) {
   uint32_t p[2 * N];
   mul_full<N>(p, a.m, b.m);
   round_prod<N>(r, p, a.e + b.e, a.s ^ b.s);
+}
+
+/* r = round(a * b).  From N = 4 limbs up only the upper columns are
+ * computed (about half the partial products).  With X the 64 bits under the
+ * mantissa (words N-1 and N-2 of T after the normalisation shift), the exact
+ * product has X + lambda there, 0 <= lambda < 2^39: X <= 2^63 - 2^39 - 1
+ * rounds down and X > 2^63 rounds up (a carry into the mantissa gives the
+ * same result) whatever lambda is.  X in between -- about 2^-25 of random
+ * operands, exact ties included -- rounds the full product instead. */
+template <int N>
+MPB_HD void mul(fval<N> &r, const fval<N> &a, const fval<N> &b) {
+  uint32_t p[2 * N];
+  if (N >= 4) {
+    mul_high<N>(p, a.m, b.m);
+    MPB_UNROLL
+    for (int i = 0; i < N - 2; ++i) p[i] = 0u;
+    const uint32_t sh = (p[2 * N - 1] >> 31) ^ 1u;
+    const uint64_t X = ((((uint64_t)p[N - 1]) << 32) | p[N - 2]) << sh;
+    const bool sure = X <= (1ull << 63) - (1ull << 39) - 1ull || X > (1ull << 63);
+    if (sure)
+      round_prod<N>(r, p, a.e + b.e, a.s ^ b.s);
+    else
+      mul_full_round<N>(r, a, b);
+  } else {
+    mul_full<N>(p, a.m, b.m);
+    round_prod<N>(r, p, a.e + b.e, a.s ^ b.s);
+  }
   if (is_zero(a) || is_zero(b)) set_zero(r);
 }
 

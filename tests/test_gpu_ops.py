@@ -60,6 +60,20 @@ def test_binops_real(orc, mpb, prec):
     assert bad == 0, f"fma PB={prec}: {bad} mismatches, first at {first}"
 
 
+@pytest.mark.parametrize("prec", (128, 256, 512, 1024, 2048))
+def test_mul_uncertain_window(orc, mpb, prec):
+    """Products next to a rounding midpoint (exact ties included): the kernel
+    must fall back from the upper-column product to the full one."""
+    from test_host_dropin import window_aos
+
+    A, B = window_aos(prec, 2000, prec + 1)
+    M = A.shape[0]
+    r = mpb.empty(prec, M)
+    mpb.binop(prec, 0, M, dvec(prec, A), dvec(prec, B), r)
+    bad, first = orc.mismatches(prec, hvec(prec, r, M), orc.binop("mul", prec, A, B, "mp"))
+    assert bad == 0, f"PB={prec}: {bad} mismatches, first at {first}"
+
+
 @pytest.mark.parametrize("prec", PRECS)
 def test_binops_complex(orc, mpb, prec):
     M = 30000 if prec <= 1024 else 6000

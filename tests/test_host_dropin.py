@@ -46,6 +46,70 @@ def test_complex_ops(orc, mpb, prec):
         assert bad == 0, f"{kind} PB={prec}: first mismatch {first}"
 
 
+def window_operands(prec, count, seed):
+    """(limbs_a, limbs_b) pairs of prec-bit significands whose product cannot be
+    rounded from the upper columns of the limb product alone: the 64 bits under
+    the mantissa of the truncated product lie within 2^39 below the midpoint,
+    so the full product decides.  a = 2^(P-1) + small odd, b with a bit
+    pattern right under the rounding position: 1000..0 or 0111..1 over 29 bits
+    (half the time with nothing below: exact ties), or 1 followed by 63 zeros
+    with random bits below, where the truncated product is an exact tie and only
+    the omitted low pairs show that the product lies above the midpoint."""
+    import random
+
+    P, N = prec, prec // 32
+    rng = random.Random(seed)
+    limbs = lambda v: [(v >> (32 * i)) & 0xFFFFFFFF for i in range(N)]  # noqa: E731
+    out = []
+    while len(out) < count:
+        M = (1 << (P - 1)) | rng.getrandbits(P - 1)
+        if rng.random() < 0.5:
+            A = (1 << (P - 1)) + 1
+            M = (M & ~(((1 << 64) - 1) << (P - 65))) | ((1 << 63) << (P - 65))
+        else:
+            A = (1 << (P - 1)) + rng.choice((1, 3, 5))
+            pat = rng.choice((1 << 28, (1 << 28) - 1))
+            M = (M & ~(((1 << 29) - 1) << (P - 30))) | (pat << (P - 30))
+            if rng.random() < 0.5:
+                M &= ~((1 << (P - 30)) - 1)
+        a, b = limbs(A), limbs(M)
+        if rng.random() < 0.5:
+            a, b = b, a
+        c0 = sum(a[i] * b[N - 2 - i] for i in range(N - 1))
+        c1 = sum(a[i] * b[N - 1 - i] for i in range(N))
+        sh = 1 - ((A * M) >> (2 * P - 1))
+        X = (((c0 + (c1 << 32)) & ((1 << 64) - 1)) << sh) & ((1 << 64) - 1)
+        if (1 << 63) - (1 << 39) - 1 < X <= (1 << 63):
+            out.append((a, b))
+    return out
+
+
+def window_aos(prec, count, seed):
+    from mpc_cuda_b200 import layout
+
+    pairs = window_operands(prec, count, seed)
+    rng = np.random.default_rng(seed)
+
+    def heads():
+        return ((rng.integers(-40, 40, count).astype(np.int64) << 1) | rng.integers(0, 2, count)).astype(np.uint32)
+
+    A = layout.aos_from_parts(prec, np.array([p[0] for p in pairs], np.uint32), heads())
+    B = layout.aos_from_parts(prec, np.array([p[1] for p in pairs], np.uint32), heads())
+    return A, B
+
+
+@pytest.mark.parametrize("prec", (128, 256, 512, 1024, 2048))
+def test_mul_uncertain_window_takes_full_product(orc, mpb, prec):
+    """Products whose rounding the upper half of the limb product cannot
+    decide (near and exact ties) must still round like MPFR."""
+    H = mpb.host_lib()
+    A, B = window_aos(prec, 200, prec)
+    R = orc.empty(prec, A.shape[0])
+    assert H.mpbh_binop(prec, 0, A.shape[0], _p(A), _p(B), _p(R)) == 0
+    bad, first = orc.mismatches(prec, R, orc.binop("mul", prec, A, B, "mp"))
+    assert bad == 0, f"PB={prec}: {bad} mismatches, first at {first}"
+
+
 def _negate_complex(orc, prec, Z):
     """-Z for complex AoS elements (flip both components' sign words)."""
     es = orc.elem_bytes(prec)
