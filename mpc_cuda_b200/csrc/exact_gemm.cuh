@@ -487,41 +487,43 @@ __device__ __forceinline__ bool round_words(fval<N> &r, uint32_t (&v)[W], long l
   return ok;
 }
 
-/* round_words for a sum held in shared memory (this thread's W words at
- * sv[0..W), stride 1): the words are negated in place when negative, then only
- * the N + 2 words under the leading bit are read (runtime index from the top
- * word) and the rest is OR-ed into the sticky bit, so no register array of W
- * words and no shift network over it is needed.  Same result and the same
- * certification as round_words. */
+/* round_words for a sum held in registers v[0..W) with a shared-memory slot
+ * sv[0..W) for this thread: the sign, the magnitude (negation with one carry
+ * chain), the top nonzero word and the lowest nonzero word come from the
+ * registers; the magnitude words then go to sv once, and only the N + 2
+ * words under the leading bit are read back, at indices counted from the top
+ * word (no shift network over all W words).  Everything below those words
+ * only matters as the sticky bit, which is "the lowest nonzero word lies
+ * below them".  Same result and certification as round_words. */
 template <int N, int W>
-__device__ __forceinline__ bool round_smem(fval<N> &r, uint32_t *sv, long lsb_exp, long cert) {
+__device__ __forceinline__ bool round_regs(fval<N> &r, uint32_t (&v)[W], uint32_t *sv, long lsb_exp, long cert) {
   static_assert(W >= N + 2, "word window too small");
-  const uint32_t neg = sv[W - 1] >> 31;
-  if (neg) {
-    uint32_t c = 1;
+  const uint32_t neg = v[W - 1] >> 31;
+  {
+    const uint32_t msk = 0u - neg;
+    uint32_t cf = 0;
+    cc_set(neg, cf);
 #pragma unroll
-    for (int w = 0; w < W; ++w) {
-      const uint32_t t = ~sv[w] + c;
-      c = (c && t == 0) ? 1u : 0u;
-      sv[w] = t;
-    }
+    for (int w = 0; w < W; ++w) v[w] = addc_cc(v[w] ^ msk, 0u, cf);
   }
-  int top = -1;
+  int top = -1, low = W;
 #pragma unroll
-  for (int w = 0; w < W; ++w) top = sv[w] != 0u ? w : top;
+  for (int w = 0; w < W; ++w) top = v[w] != 0u ? w : top;
+#pragma unroll
+  for (int w = W - 1; w >= 0; --w) low = v[w] != 0u ? w : low;
   if (top < 0) {
     set_zero(r);
     return cert < 0;
   }
+#pragma unroll
+  for (int w = 0; w < W; ++w) sv[w] = v[w];
   auto word = [&](int i) -> uint32_t { return i >= 0 ? sv[i] : 0u; };
   const uint32_t lr = clz32(sv[top]) & 31u;
 #pragma unroll
   for (int i = 0; i < N; ++i) r.m[N - 1 - i] = fshl(word(top - i - 1), word(top - i), lr);
   const uint32_t g = fshl(word(top - N - 1), word(top - N), lr);
   const uint32_t nx = fshl(word(top - N - 2), word(top - N - 1), lr);
-  uint32_t st = (g << 1) | (word(top - N - 1) << lr);
-#pragma unroll
-  for (int w = 0; w < W; ++w) st |= (w <= top - N - 2) ? sv[w] : 0u;
+  const uint32_t st = (g << 1) | (word(top - N - 1) << lr) | (low <= top - N - 2 ? 1u : 0u);
   const long msb = 32L * top + 31 - lr;
   bool ok = true;
   if (cert >= 0) {
@@ -570,8 +572,13 @@ __device__ __forceinline__ bool pass_entry(const RoundPass &rp, int m, int n, si
     return rp.ef[idx] != 0;
   }
   idx = u;
-  i = (int)(u / n);
-  j = (int)(u % n);
+  if (u < (1ull << 32)) { /* 32-bit division when the index fits */
+    i = (int)((uint32_t)u / (uint32_t)n);
+    j = (int)((uint32_t)u - (uint32_t)i * (uint32_t)n);
+  } else {
+    i = (int)(u / n);
+    j = (int)(u % n);
+  }
   return true;
 }
 __device__ __forceinline__ size_t pass_total(const RoundPass &rp, int m, int n) {
@@ -587,8 +594,8 @@ __device__ __forceinline__ void mark_tile(const RoundPass &rp, int i, int j) {
  * streamed into 32-bit words with an int64 carry -- plane d_first + j lands
  * in word j/4, byte j%4.  The words hold the sum divided by 256^d_first, so
  * the LSB exponent and the certification bound move up by 8 d_first bits
- * instead of the words moving.  The words then go to the thread's slot in
- * shared memory, where round_smem reads only the ones it needs.  Complex
+ * instead of the words moving.  round_regs rounds them, reading the few
+ * words under the leading bit from the thread's shared-memory slot.  Complex
  * outputs read each product's planes once and form both components:
  * re = T0 - T1, im = T2 - T0 - T1.  Every loop is unrolled at compile time. */
 template <int N, int XL, bool CPLX>
@@ -628,12 +635,16 @@ __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
       int32_t t0v[BATCH], t1v[CPLX ? BATCH : 1], t2v[CPLX ? BATCH : 1];
 #pragma unroll
       for (int jj = 0; jj < BATCH; ++jj) {
+        /* unconditional loads (a plane past the last one re-reads the last,
+         * then counts as 0), so they can all be issued before any is used */
         const bool in = j0 + jj < nl;
-        const size_t off = (size_t)(j0 + jj) * plane;
-        t0v[jj] = in ? __ldcs(base + off) : 0;
+        const size_t off = (size_t)min(j0 + jj, nl - 1) * plane;
+        const int32_t x0 = base[off];
+        t0v[jj] = in ? x0 : 0;
         if (CPLX) {
-          t1v[jj] = in ? __ldcs(base + qstride + off) : 0;
-          t2v[jj] = in ? __ldcs(base + 2 * qstride + off) : 0;
+          const int32_t x1 = base[qstride + off], x2 = base[2 * qstride + off];
+          t1v[jj] = in ? x1 : 0;
+          t2v[jj] = in ? x2 : 0;
         }
       }
 #pragma unroll
@@ -662,21 +673,14 @@ __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
         }
       }
     }
-    /* words to this thread's shared-memory slot only now, so that no store
-     * separates the batches of plane loads above */
-#pragma unroll
-    for (int w = 0; w < QJ; ++w) {
-      svr[w] = vr[w];
-      if (CPLX) svi[w] = vi[w];
-    }
     const long lsb = (long)rowE[i] + colE[j] - 2L * (32 * N) - 2L * SP + 8L * rp.d_first;
     /* an all-zero row or column has all-zero digits: its sum is exactly 0 */
     const long cert =
         (rowE[i] == kExpZero || colE[j] == kExpZero || rp.cert < 0) ? -1 : rp.cert - 8L * rp.d_first;
     fval<N> re;
-    bool ok = round_smem<N, QJ>(re, svr, lsb, cert);
+    bool ok = round_regs<N, QJ>(re, vr, svr, lsb, cert);
     fval<N> im;
-    if (CPLX) ok = round_smem<N, QJ>(im, svi, lsb, cert) && ok;
+    if (CPLX) ok = round_regs<N, QJ>(im, *reinterpret_cast<uint32_t(*)[QJ]>(vi), svi, lsb, cert) && ok;
     if (!rp.flagged_only) {
       rp.ef[idx] = ok ? 0 : 1;
       if (!ok) {
