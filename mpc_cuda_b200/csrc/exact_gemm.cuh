@@ -600,7 +600,7 @@ __device__ __forceinline__ void mark_tile(const RoundPass &rp, int i, int j) {
  * re = T0 - T1, im = T2 - T0 - T1.  Every loop is unrolled at compile time. */
 template <int N, int XL, bool CPLX>
 __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
-                                  round_geo<N, XL>::template threads<CPLX>() == 128 ? 5 : 10)
+                                  round_geo<N, XL>::template threads<CPLX>() == 128 ? 4 : 8)
     k_exact_round(int m, int n, int S, int SP, const int32_t *__restrict__ D, const int32_t *rowE, const int32_t *colE,
                   const uint8_t *rowF, const uint8_t *colF, uint8_t *C, size_t ldc, RoundPass rp) {
   constexpr int J = round_geo<N, XL>::J;
