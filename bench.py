@@ -136,9 +136,10 @@ def imad_peak(stream_ptr):
 
 
 def rounded_product_imads(N):
-    """32-bit multiply-adds (lo + hi per limb pair) of one correctly rounded
-    N-limb product as the engine computes it: from N = 4 up only the columns
-    N-2 .. 2N-2 of the limb product (the rare full-product case aside)."""
+    """32-bit multiply-adds (lo + hi per limb pair) of one N-limb product as the
+    engine computes it for a rounded product or a certified fmms: from N = 4
+    up only the columns N-2 .. 2N-2 of the limb product (the rare exact case
+    aside)."""
     if N < 4:
         return 2 * N * N
     return 2 * ((N - 1) + N + N * (N - 1) // 2)
@@ -228,8 +229,8 @@ class AxpyWorkload:
 
     def roofline(self, kernel_s, peaks, imad_ops_s):
         N = self.prec // 32
-        # complex: 4 exact (full) products; real: one rounded (upper-column) product
-        imad_per_unit = 4 * 2 * N * N if self.cplx else rounded_product_imads(N)
+        # complex: 4 upper-column products (two certified fmms); real: one rounded product
+        imad_per_unit = (4 if self.cplx else 1) * rounded_product_imads(N)
         bytes_per_unit = 3 * self.elem_bytes
         imad = imad_per_unit * self.n / kernel_s
         gbs = bytes_per_unit * self.n / kernel_s / 1e9
@@ -472,6 +473,8 @@ class GemvBatchWorkload:
             d = {k: dev_from(layout.aos_to_vec(p, a), device) for k, a in zip(("A", "x", "y"), (A, x, y))}
             d["yo"] = torch.zeros_like(d["y"])
             self.dev[p] = d
+            if not getattr(self, "with_e2e", True):
+                continue
             self.pin[p] = {"A": pinned_from(A), "x": pinned_from(x), "y": pinned_from(y),
                            "yo": [torch.empty(y.size, dtype=torch.uint8).pin_memory() for _ in range(2)]}
             self.stage[p] = {k: [torch.empty(a.size, dtype=torch.uint8, device=device) for _ in range(2)]
@@ -734,6 +737,7 @@ def run_gpu(args):
         return float(t.item())
 
     wl = WORKLOADS[args.workload]()
+    wl.with_e2e = not args.no_e2e
     wl.setup(rank, device)
     stream = torch.cuda.current_stream(device)
     sp = stream.cuda_stream
@@ -769,24 +773,26 @@ def run_gpu(args):
     kernel_s = ms / args.steps / 1e3
 
     # end to end through the C ABI from host AoS buffers
-    pipe = E2EPipeline(wl, stream)
-    pipe.start()
-    for i in range(max(1, args.warmup)):
-        pipe.step(i)
-    pipe.finish()
-    torch.cuda.synchronize()
-    barrier()
-    e2 = torch.cuda.Event(enable_timing=True)
-    e3 = torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    pipe.start()
-    for i in range(args.steps):
-        pipe.step(i)
-    pipe.finish()
-    e3.record(stream)
-    torch.cuda.synchronize()
-    ms_e2e = max_over_ranks(e2.elapsed_time(e3))
-    barrier()
+    ms_e2e = None
+    if not args.no_e2e:
+        pipe = E2EPipeline(wl, stream)
+        pipe.start()
+        for i in range(max(1, args.warmup)):
+            pipe.step(i)
+        pipe.finish()
+        torch.cuda.synchronize()
+        barrier()
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        pipe.start()
+        for i in range(args.steps):
+            pipe.step(i)
+        pipe.finish()
+        e3.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = max_over_ranks(e2.elapsed_time(e3))
+        barrier()
 
     units = wl.units() * world * args.steps
     if rank == 0:
@@ -805,10 +811,11 @@ def run_gpu(args):
             "data": "synthetic", "config": {**wl.config(), "parallelism": f"{world} independent shard(s), "
                                                                           "no collective"},
             "roofline": roof, "cpu_baseline": cpu,
-            "e2e": {"value": units / (ms_e2e / 1e3), "unit": "mp-FMA/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps,
-                    "path": "pinned host AoS -> H2D -> mpb_pack_aos -> kernel -> mpb_unpack_aos -> D2H, "
-                            "double-buffered: H2D, compute and D2H of consecutive steps overlap"},
+            "e2e": None if ms_e2e is None else {
+                "value": units / (ms_e2e / 1e3), "unit": "mp-FMA/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps,
+                "path": "pinned host AoS -> H2D -> mpb_pack_aos -> kernel -> mpb_unpack_aos -> D2H, "
+                        "double-buffered: H2D, compute and D2H of consecutive steps overlap"},
             "gpu_launches": wl.launches_per_step * args.steps,
             "gpu_launches_e2e": wl.e2e_launches_per_step * args.steps,
             "clocks": clk,
@@ -835,7 +842,14 @@ def main():
     ap.add_argument("--impl", choices=("mpb", "reference"), default="mpb")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--problems", type=int, default=None,
+                    help="gemv_batch only: number of problems (profiling runs on a small case)")
     args = ap.parse_args()
+    if args.problems is not None:
+        if args.workload != "gemv_batch" or args.problems < 1:
+            ap.error("--problems applies to --workload gemv_batch, with a positive count")
+        WORKLOADS["gemv_batch"] = lambda: GemvBatchWorkload("gemv_batch", args.problems, 0x5EED4)
     if args.warmup < 3:
         args.warmup = 3
     if args.steps is None:

@@ -14,7 +14,7 @@
  *   mul          round(a*b)                (upper half of the N x N product, certified)
  *   add_round    round(x + y)              (x, y exact NX-limb terms, result NM limbs)
  *   fma          round(a*b + c)            (single rounding)
- *   fmms/fmma    round(a*b -/+ c*d)        (single rounding; complex multiply)
+ *   fmms/fmma    round(a*b -/+ c*d)        (single rounding, certified upper-column products; complex multiply)
  *   sum3_round   round(t1 + t2 + t3)       (three exact terms; complex fma: cfma)
  * Zero is unsigned (+0), as in cu_freal (cu_freal.cuh:79-81 of mpc_cuda).
  *
@@ -353,8 +353,14 @@ struct log2_ceil<1> {
   static constexpr int v = 0;
 };
 
-template <int NX, int NM, bool kVote = false>
-MPB_HD void add_round(fval<NM> &r, const uint32_t *xm, int32_t xe, uint32_t xs,
+/* kCertBits > 0: the terms are known only to within a total error below
+ * 2^(ea - kCertBits) (ea = the larger term exponent), and the function also
+ * reports whether every value within that error rounds to the same r: the
+ * error must stay under a quarter ULP of r and the bits under the mantissa,
+ * read as the 64-bit fraction G, clear of the midpoint by more than it (a
+ * zero sum never certifies).  Without it the return value is true. */
+template <int NX, int NM, bool kVote = false, int kCertBits = 0>
+MPB_HD bool add_round(fval<NM> &r, const uint32_t *xm, int32_t xe, uint32_t xs,
                       const uint32_t *ym, int32_t ye, uint32_t ys) {
   constexpr int W = NX + 2;
   constexpr int KQ = log2_ceil<W + 1>::v; /* limb-shift stages: 2^KQ > W */
@@ -463,10 +469,20 @@ MPB_HD void add_round(fval<NM> &r, const uint32_t *xm, int32_t xe, uint32_t xs,
   MPB_UNROLL
   for (int i = 0; i < W - NM - 1; ++i) st |= D[i];
   int32_t e = ea + (int32_t)cs - (int32_t)(32u * lq + lr);
+  bool ok = true;
+  if (kCertBits > 0) {
+    static_assert(W - NM - 2 >= 0, "no word under the guard word");
+    const int64_t t = ((int64_t)ea - kCertBits) - ((int64_t)e - 32 * NM); /* log2 of the error in ULPs */
+    const uint64_t G = ((uint64_t)g << 32) | D[W - NM - 2];
+    const uint64_t thr = (t < -64) ? 1ull : (1ull << (64 + (t < -3 ? t : -3)));
+    const uint64_t half = 1ull << 63;
+    ok = !zero && t <= -3 && (G <= half - thr - 1 || G > half + thr);
+  }
   rndn<NM>(r.m, e, g >> 31, st);
   r.e = e;
   r.s = s;
   if (zero) set_zero(r);
+  return ok;
 }
 
 /* r = round(x + y), r = round(x - y) */
@@ -496,15 +512,52 @@ MPB_HD void fma(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c
 /* round(a*b - c*d) and round(a*b + c*d), one rounding each (MPFR
  * mpfr_fmms / mpfr_fmma semantics; the exact-intermediate complex product
  * of MPC_RNDNN, mpc_cuda cu_fcomplex.cuh:91-96) */
+template <int N>
+MPB_NOINLINE void fmms_full(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c, const fval<N> &d,
+                            uint32_t negate_cd) {
+  uint32_t p1[2 * N], p2[2 * N];
+  int32_t e1, e2;
+  mul_exact_norm<N>(p1, e1, a, b);
+  mul_exact_norm<N>(p2, e2, c, d);
+  add_round<2 * N, N>(r, p1, e1, a.s ^ b.s, p2, e2, c.s ^ d.s ^ negate_cd);
+}
+
+/* upper columns of a*b (mul_high), normalised like mul_exact_norm; zero stays 0 */
+template <int N>
+MPB_HD void mul_high_norm(uint32_t *p, int32_t &e, const fval<N> &a, const fval<N> &b) {
+  mul_high<N>(p, a.m, b.m);
+  MPB_UNROLL
+  for (int i = 0; i < N - 2; ++i) p[i] = 0u;
+  const uint32_t sh = (p[2 * N - 1] >> 31) ^ 1u;
+  MPB_UNROLL
+  for (int i = 2 * N - 1; i > 0; --i) p[i] = fshl(p[i - 1], p[i], sh);
+  p[0] <<= sh;
+  e = a.e + b.e - (int32_t)sh;
+  if (is_zero(a) || is_zero(b)) e = kExpZero;
+}
+
+/* From N = 4 limbs up both products are taken from their upper columns
+ * only: each then misses less than N 2^(32(N-1)) units of its lowest word,
+ * i.e. below 2^(e_i - 32N - 25) for |product| < 2^(e_i), so the sum is off by
+ * less than 2^(e_max - 32N - 24).  add_round certifies the rounding against
+ * that (it fails under heavy cancellation -- more than about 20 bits -- or
+ * next to a midpoint), and the exact products decide otherwise. */
 template <int N, bool kVote = false>
 MPB_HD void fmms(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c,
                  const fval<N> &d, uint32_t negate_cd = 1u) {
   uint32_t p1[2 * N], p2[2 * N];
   int32_t e1, e2;
-  mul_exact_norm<N>(p1, e1, a, b);
-  mul_exact_norm<N>(p2, e2, c, d);
   uint32_t s2 = c.s ^ d.s ^ negate_cd;
-  add_round<2 * N, N, kVote>(r, p1, e1, a.s ^ b.s, p2, e2, s2);
+  if (N >= 4) {
+    mul_high_norm<N>(p1, e1, a, b);
+    mul_high_norm<N>(p2, e2, c, d);
+    const bool ok = add_round<2 * N, N, kVote, 32 * N + 24>(r, p1, e1, a.s ^ b.s, p2, e2, s2);
+    if (!ok && !(e1 == kExpZero && e2 == kExpZero)) fmms_full<N>(r, a, b, c, d, negate_cd);
+  } else {
+    mul_exact_norm<N>(p1, e1, a, b);
+    mul_exact_norm<N>(p2, e2, c, d);
+    add_round<2 * N, N, kVote>(r, p1, e1, a.s ^ b.s, p2, e2, s2);
+  }
 }
 template <int N, bool kVote = false>
 MPB_HD void fmma(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c,

@@ -74,6 +74,20 @@ def test_mul_uncertain_window(orc, mpb, prec):
     assert bad == 0, f"PB={prec}: {bad} mismatches, first at {first}"
 
 
+@pytest.mark.parametrize("prec", (128, 256, 512, 1024, 2048))
+def test_cmul_cancellation(orc, mpb, prec):
+    """Complex products whose real part cancels exactly or down to ~2^-PB:
+    the kernel must fall back from upper-column products to exact ones."""
+    from test_host_dropin import cancelling_complex_pairs
+
+    A, B = cancelling_complex_pairs(orc, prec, 4000, 0x7171 + prec)
+    M = A.shape[0]
+    r = mpb.empty(prec, M, True)
+    mpb.binop(prec, 0, M, dvec(prec, A, True), dvec(prec, B, True), r, cplx=True)
+    bad, first = orc.mismatches(prec, hvec(prec, r, M, True), orc.binop("cmul", prec, A, B, "mp"), True)
+    assert bad == 0, f"PB={prec}: {bad} mismatches, first at {first}"
+
+
 @pytest.mark.parametrize("prec", PRECS)
 def test_binops_complex(orc, mpb, prec):
     M = 30000 if prec <= 1024 else 6000

@@ -110,6 +110,30 @@ def test_mul_uncertain_window_takes_full_product(orc, mpb, prec):
     assert bad == 0, f"PB={prec}: {bad} mismatches, first at {first}"
 
 
+def cancelling_complex_pairs(orc, prec, M, seed):
+    """Complex (a, b) pairs whose real part a_r b_r - a_i b_i cancels: b = (y, x)
+    for a = (x, y) gives exactly 0, and with the last bit of x flipped in b
+    the real part is ~2^-PB below its terms.  The complex multiply cannot
+    round these from upper-column products and must use the exact ones."""
+    es = orc.elem_bytes(prec)
+    A, _ = orc.gen_pairs(prec, M, seed, cplx=True)
+    B = A.copy()
+    B[:, :es], B[:, es:] = A[:, es:], A[:, :es]
+    sb = 64 * (-(-prec // 64)) - prec  # zero padding bits under the significand
+    B[1::2, es + 16 + sb // 8] ^= 1 << (sb % 8)  # last significand bit of b's imaginary part (x), every other pair
+    return A, B
+
+
+@pytest.mark.parametrize("prec", (128, 160, 256, 512, 1024, 2048))
+def test_cmul_cancellation_uses_exact_products(orc, mpb, prec):
+    H = mpb.host_lib()
+    A, B = cancelling_complex_pairs(orc, prec, 600, 0x5151 + prec)
+    R = orc.empty(prec, A.shape[0], True)
+    assert H.mpbh_cbinop(prec, 0, A.shape[0], _p(A), _p(B), _p(R)) == 0
+    bad, first = orc.mismatches(prec, R, orc.binop("cmul", prec, A, B, "mp"), True)
+    assert bad == 0, f"PB={prec}: {bad} mismatches, first at {first}"
+
+
 def _negate_complex(orc, prec, Z):
     """-Z for complex AoS elements (flip both components' sign words)."""
     es = orc.elem_bytes(prec)
