@@ -286,38 +286,44 @@ MPB_HD void mul_high(uint32_t *p, const uint32_t *a, const uint32_t *b) {
 
 /* the full product and its rounding, out of line: the rare case of mul */
 template <int N>
-MPB_NOINLINE void mul_full_round(fval<N> &r, const fval<N> &a, const fval<N> &b) {
+MPB_NOINLINE void mul_full_round(fval<N> &r, const fval<N> &a, const uint32_t *bm, int32_t be, uint32_t bs) {
   uint32_t p[2 * N];
-  mul_full<N>(p, a.m, b.m);
-  round_prod<N>(r, p, a.e + b.e, a.s ^ b.s);
+  mul_full<N>(p, a.m, bm);
+  round_prod<N>(r, p, a.e + be, a.s ^ bs);
 }
 
-/* r = round(a * b).  From N = 4 limbs up only the upper columns are
- * computed (about half the partial products).  With X the 64 bits under the
+/* r = round(a * b), b given by its limbs (which may live in shared memory:
+ * mul_high reads them one at a time) and exponent / sign.  From N = 4 limbs
+ * up only the upper columns are computed (about half the partial products).  With X the 64 bits under the
  * mantissa (words N-1 and N-2 of T after the normalisation shift), the exact
  * product has X + lambda there, 0 <= lambda < 2^39: X <= 2^63 - 2^39 - 1
  * rounds down and X > 2^63 rounds up (a carry into the mantissa gives the
  * same result) whatever lambda is.  X in between -- about 2^-25 of random
  * operands, exact ties included -- rounds the full product instead. */
 template <int N>
-MPB_HD void mul(fval<N> &r, const fval<N> &a, const fval<N> &b) {
+MPB_HD void mul_limbs(fval<N> &r, const fval<N> &a, const uint32_t *bm, int32_t be, uint32_t bs) {
   uint32_t p[2 * N];
   if (N >= 4) {
-    mul_high<N>(p, a.m, b.m);
+    mul_high<N>(p, a.m, bm);
     MPB_UNROLL
     for (int i = 0; i < N - 2; ++i) p[i] = 0u;
     const uint32_t sh = (p[2 * N - 1] >> 31) ^ 1u;
     const uint64_t X = ((((uint64_t)p[N - 1]) << 32) | p[N - 2]) << sh;
     const bool sure = X <= (1ull << 63) - (1ull << 39) - 1ull || X > (1ull << 63);
     if (sure)
-      round_prod<N>(r, p, a.e + b.e, a.s ^ b.s);
+      round_prod<N>(r, p, a.e + be, a.s ^ bs);
     else
-      mul_full_round<N>(r, a, b);
+      mul_full_round<N>(r, a, bm, be, bs);
   } else {
-    mul_full<N>(p, a.m, b.m);
-    round_prod<N>(r, p, a.e + b.e, a.s ^ b.s);
+    mul_full<N>(p, a.m, bm);
+    round_prod<N>(r, p, a.e + be, a.s ^ bs);
   }
-  if (is_zero(a) || is_zero(b)) set_zero(r);
+  if (is_zero(a) || be == kExpZero) set_zero(r);
+}
+/* the same with b as a value */
+template <int N>
+MPB_HD void mul(fval<N> &r, const fval<N> &a, const fval<N> &b) {
+  mul_limbs<N>(r, a, b.m, b.e, b.s);
 }
 
 /* exact product, normalised so that bit 31 of p[2N-1] is set (zero stays 0) */
