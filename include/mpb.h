@@ -87,6 +87,13 @@ int mpb_to_double(int prec, size_t n, const void *vec, double *d, void *stream);
 int mpb_binop_r(int prec, int op, size_t n, const void *a, const void *b, void *r, void *stream);
 /* r[i] = round(a[i]*b[i] + c[i]), one rounding (mpfr_fma; no counterpart in the reference) */
 int mpb_fma_r(int prec, size_t n, const void *a, const void *b, const void *c, void *r, void *stream);
+/* r[i] = round(a[i] / b[i]) and r[i] = round(sqrt(a[i])), one rounding each
+ * (mpfr_div / mpfr_sqrt; the drop-in cu_fdiv / cu_sqrt).  They replace the
+ * reference's faithful cu_fdiv / cu_sqrt (include/mpc_cuda/cu_fmath.cuh:67-75,
+ * 92-100) with correctly rounded ones.  b[i] = 0 or a[i] < 0 gives 0 (the
+ * format has no infinities or NaN). */
+int mpb_div_r(int prec, size_t n, const void *a, const void *b, void *r, void *stream);
+int mpb_sqrt_r(int prec, size_t n, const void *a, void *r, void *stream);
 /* complex r[i] = a[i]*b[i] + c[i], one rounding per component from exact
  * products (mpc_fma; the drop-in cu_cfma; no counterpart in the reference) */
 int mpb_fma_c(int prec, size_t n, const void *a, const void *b, const void *c, void *r, void *stream);

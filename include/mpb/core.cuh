@@ -16,6 +16,7 @@
  *   fma          round(a*b + c)            (single rounding)
  *   fmms/fmma    round(a*b -/+ c*d)        (single rounding, certified upper-column products; complex multiply)
  *   sum3_round   round(t1 + t2 + t3)       (three exact terms; complex fma: cfma)
+ *   div, sqrt_   round(a/b), round(sqrt(a)) (exact long division / integer square root)
  * Zero is unsigned (+0), as in cu_freal (cu_freal.cuh:79-81 of mpc_cuda).
  *
  * B200 design points:
@@ -36,6 +37,7 @@
 #ifndef MPB_CORE_CUH
 #define MPB_CORE_CUH
 
+#include <math.h>
 #include <stdint.h>
 
 #if defined(__CUDACC__)
@@ -779,6 +781,160 @@ MPB_HD void cfma(fval<N> &rr, fval<N> &ri, const fval<N> &ar, const fval<N> &ai,
     else
       rr = r;
   }
+}
+
+/* ------------------------------------------------------------------ *
+ * Division and square root, correctly rounded (MPFR mpfr_div / mpfr_sqrt)
+ * ------------------------------------------------------------------ */
+/* Long division of limb integers (Knuth's algorithm D, base 2^32), every
+ * index known at compile time: q[0 .. NU-NV) = floor(U / V) and u[0 .. NV)
+ * becomes U mod V.  V must be normalised (top bit of v[NV-1] set) and
+ * U < V * 2^(32 (NU - NV)).  Each quotient limb is estimated from the top two
+ * remainder limbs and the top divisor limb, corrected with the second
+ * divisor limb (at most twice), and fixed by one add-back when the
+ * multiply-subtract goes negative. */
+template <int NU, int NV>
+MPB_HD void divmod_limbs(uint32_t *q, uint32_t *u, const uint32_t *v) {
+  const uint64_t v1 = v[NV - 1];
+  const uint64_t v2 = NV >= 2 ? v[NV - 2 >= 0 ? NV - 2 : 0] : 0u;
+  MPB_UNROLL
+  for (int j = NU - NV - 1; j >= 0; --j) {
+    const uint64_t num = ((uint64_t)u[j + NV] << 32) | u[j + NV - 1];
+    uint64_t qh = num / v1, rh = num - qh * v1;
+    const uint64_t u3 = (j + NV - 2 >= 0) ? u[j + NV - 2 >= 0 ? j + NV - 2 : 0] : 0u;
+    MPB_UNROLL
+    for (int c = 0; c < 2; ++c) {
+      if (rh < (1ull << 32) && (qh >= (1ull << 32) || qh * v2 > ((rh << 32) | u3))) {
+        --qh;
+        rh += v1;
+      }
+    }
+    /* u[j .. j+NV] -= qh * v */
+    uint64_t carry = 0;
+    uint32_t borrow = 0;
+    MPB_UNROLL
+    for (int i = 0; i < NV; ++i) {
+      const uint64_t p = qh * v[i] + carry;
+      carry = p >> 32;
+      const uint64_t t = (uint64_t)u[j + i] - (uint32_t)p - borrow;
+      u[j + i] = (uint32_t)t;
+      borrow = (uint32_t)(t >> 63);
+    }
+    const uint64_t top = (uint64_t)u[j + NV] - carry - borrow;
+    u[j + NV] = (uint32_t)top;
+    if (top >> 63) { /* estimate one too large: add v back */
+      --qh;
+      uint64_t c = 0;
+      MPB_UNROLL
+      for (int i = 0; i < NV; ++i) {
+        const uint64_t t = (uint64_t)u[j + i] + v[i] + c;
+        u[j + i] = (uint32_t)t;
+        c = t >> 32;
+      }
+      u[j + NV] += (uint32_t)c;
+    }
+    q[j] = (uint32_t)qh;
+  }
+}
+
+/* r = round(a / b), one rounding.  With A, B the significands (a = A 2^(ea-32N)),
+ * Q = floor(A 2^(32(N+1)) / B) has 32(N+1) or 32(N+1)+1 bits: the top 32N
+ * are the result, the next bit the round bit, the rest plus a nonzero
+ * remainder the sticky bit.  b = 0 has no result in this format (no
+ * infinities): r is 0. */
+template <int N>
+MPB_HD void div(fval<N> &r, const fval<N> &a, const fval<N> &b) {
+  if (is_zero(a) || is_zero(b)) { /* no integer division by a zero divisor */
+    set_zero(r);
+    return;
+  }
+  uint32_t u[2 * N + 2], q[N + 2];
+  MPB_UNROLL
+  for (int i = 0; i < 2 * N + 2; ++i) u[i] = (i >= N + 1 && i <= 2 * N) ? a.m[i - N - 1] : 0u;
+  divmod_limbs<2 * N + 2, N>(q, u, b.m);
+  uint32_t rem = 0u;
+  MPB_UNROLL
+  for (int i = 0; i < N; ++i) rem |= u[i];
+  const uint32_t big = q[N + 1] & 1u; /* A >= B: one more quotient bit */
+  MPB_UNROLL
+  for (int i = 0; i < N; ++i) r.m[i] = big ? fshr(q[i + 1], q[i + 2], 1) : q[i + 1];
+  const uint32_t rb = big ? (q[1] & 1u) : (q[0] >> 31);
+  const uint32_t st = (big ? q[0] : (q[0] << 1)) | rem;
+  int32_t e = a.e - b.e + (int32_t)big;
+  rndn<N>(r.m, e, rb, st);
+  r.e = e;
+  r.s = a.s ^ b.s;
+}
+
+/* r = round(sqrt(a)), one rounding.  With a = M 2^E (E = e - 32N), X = M 2^(2K)
+ * for K = 16N + 32 (E even) or X = 2M 2^(2K) for K = 16N + 31 (E odd) lies in
+ * [2^(64N+62), 2^(64N+64)), so S = floor(sqrt(X)) has exactly 32(N+1) bits.
+ * S comes from the integer Newton iteration s <- (s + floor(X / s)) / 2,
+ * started at or above sqrt(X) from a double-precision estimate of the top
+ * 64 bits; it decreases to S and stops when it no longer decreases.  The top
+ * 32N bits of S are the result, the next the round bit, the rest plus
+ * S^2 != X the sticky bit.  Negative a has no result in this format: r is 0. */
+template <int N>
+MPB_HD void sqrt_(fval<N> &r, const fval<N> &a) {
+  constexpr int NX = 2 * N + 2, NS = N + 1;
+  if (is_zero(a) || a.s) { /* the iteration below needs a nonzero root */
+    set_zero(r);
+    return;
+  }
+  const int32_t E = a.e - 32 * N;
+  const uint32_t odd = (uint32_t)E & 1u;
+  uint32_t x[NX + 1];
+  /* X = M << (32(N+2)) (even) or M << (32(N+1) + 31) (odd) */
+  MPB_UNROLL
+  for (int i = 0; i < NX + 1; ++i) {
+    const uint32_t even_w = (i >= N + 2 && i < 2 * N + 2) ? a.m[i - N - 2] : 0u;
+    const uint32_t lo = (i >= N + 1 && i - N - 1 < N) ? a.m[i - N - 1 >= 0 ? i - N - 1 : 0] : 0u;
+    const uint32_t hi = (i >= N + 2 && i - N - 2 < N) ? a.m[i - N - 2 >= 0 ? i - N - 2 : 0] : 0u;
+    x[i] = odd ? fshl(hi, lo, 31) : even_w; /* limb of M << 31: (m[k] << 31) | (m[k-1] >> 1) */
+  }
+  /* start: t >= sqrt(top 64 bits + 1), s0 = t 2^(32N), or all ones */
+  const uint64_t T = ((uint64_t)x[NX - 1] << 32) | x[NX - 2];
+  uint64_t t = (uint64_t)sqrt((double)T) + 2u;
+  uint32_t s[NS];
+  MPB_UNROLL
+  for (int i = 0; i < NS; ++i) s[i] = (t >> 32) ? 0xffffffffu : (i == NS - 1 ? (uint32_t)t : 0u);
+  for (int it = 0; it < 64; ++it) {
+    uint32_t u[NX + 1], qq[NX + 1 - NS];
+    MPB_UNROLL
+    for (int i = 0; i < NX + 1; ++i) u[i] = x[i];
+    divmod_limbs<NX + 1, NS>(qq, u, s);
+    /* s_new = (s + q) >> 1; q has NS + 1 limbs */
+    uint32_t w[NS + 1];
+    uint32_t cf = 0;
+    w[0] = add_cc(s[0], qq[0], cf);
+    MPB_UNROLL
+    for (int i = 1; i < NS; ++i) w[i] = addc_cc(s[i], qq[i], cf);
+    w[NS] = addc(0u, qq[NS], cf);
+    uint32_t sn[NS];
+    MPB_UNROLL
+    for (int i = 0; i < NS; ++i) sn[i] = fshr(w[i], w[i + 1], 1);
+    /* continue while sn < s */
+    int cmp = 0;
+    MPB_UNROLL
+    for (int i = 0; i < NS; ++i) cmp = (sn[i] != s[i]) ? (sn[i] < s[i] ? -1 : 1) : cmp;
+    if (cmp >= 0) break;
+    MPB_UNROLL
+    for (int i = 0; i < NS; ++i) s[i] = sn[i];
+  }
+  /* sticky: S^2 != X */
+  uint32_t sq[2 * NS];
+  mul_full<NS>(sq, s, s);
+  uint32_t diff = 0u;
+  MPB_UNROLL
+  for (int i = 0; i < 2 * NS; ++i) diff |= sq[i] ^ (i < NX ? x[i] : 0u);
+  MPB_UNROLL
+  for (int i = 0; i < N; ++i) r.m[i] = s[i + 1];
+  const uint32_t rb = s[0] >> 31;
+  const uint32_t st = (s[0] << 1) | diff;
+  int32_t e = (a.e + (int32_t)odd) >> 1; /* e/2 (E even) or (e+1)/2 (E odd), exactly */
+  rndn<N>(r.m, e, rb, st);
+  r.e = e;
+  r.s = 0u;
 }
 
 /* magnitude / signed compare (-1, 0, 1) */

@@ -15,4 +15,5 @@
 #define MPB_DROPIN_UMBRELLA_CUH
 #include "mpc_cuda/cu_freal.cuh"
 #include "mpc_cuda/cu_fcomplex.cuh"
+#include "mpc_cuda/cu_fmath.cuh"
 #endif

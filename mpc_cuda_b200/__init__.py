@@ -58,6 +58,8 @@ _SIGS = {
     "mpb_binop_r": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
     "mpb_fma_r": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
     "mpb_fma_c": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
+    "mpb_div_r": ([_I, _S, _V, _V, _V, _V], C.c_int),
+    "mpb_sqrt_r": ([_I, _S, _V, _V, _V], C.c_int),
     "mpb_binop_c": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
     "mpb_axpy_r": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
     "mpb_axpy_c": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
@@ -121,6 +123,8 @@ def host_lib():
             getattr(H, name).argtypes = [_I, _I, _L, _V, _V, _V]
         H.mpbh_fma.argtypes = [_I, _L, _V, _V, _V, _V]
         H.mpbh_cfma.argtypes = [_I, _L, _V, _V, _V, _V]
+        H.mpbh_div.argtypes = [_I, _L, _V, _V, _V]
+        H.mpbh_sqrt.argtypes = [_I, _L, _V, _V]
         for name in ("mpbh_axpy_r", "mpbh_axpy_c"):
             getattr(H, name).argtypes = [_I, _L, _V, _V, _V, _V]
         H.mpbh_from_double.argtypes = [_I, _L, _V, _V]
@@ -199,6 +203,16 @@ def to_double(prec, n, vec, d, stream=None):
 
 def binop(prec, op, n, a, b, r, cplx=False, stream=None):
     _call("mpb_binop_c" if cplx else "mpb_binop_r", prec, op, n, _ptr(a), _ptr(b), _ptr(r), _stream(stream))
+
+
+def div(prec, n, a, b, r, stream=None):
+    """r = round(a / b), one rounding (0 where b is 0)."""
+    _call("mpb_div_r", prec, n, _ptr(a), _ptr(b), _ptr(r), _stream(stream))
+
+
+def sqrt(prec, n, a, r, stream=None):
+    """r = round(sqrt(a)), one rounding (0 where a < 0)."""
+    _call("mpb_sqrt_r", prec, n, _ptr(a), _ptr(r), _stream(stream))
 
 
 def fma(prec, n, a, b, c, r, cplx=False, stream=None):
@@ -322,7 +336,8 @@ class BatchGemv:
 
 __all__ = [
     "SUPPORTED", "MpbError", "aos_bytes", "tile_bytes", "vec_bytes", "build", "lib", "host_lib", "empty",
-    "empty_matrix", "pack_aos", "unpack_aos", "from_double", "to_double", "binop", "fma", "axpy", "gemv", "gemm",
+    "empty_matrix", "pack_aos", "unpack_aos", "from_double", "to_double", "binop", "fma", "div", "sqrt", "axpy",
+    "gemv", "gemm",
     "layout", "MPB_OP_MUL", "MPB_OP_ADD", "MPB_OP_SUB", "gemm_exact", "gemm_exact_workspace", "gemm_exact_info",
     "BatchGemv",
     "GemvProblem",

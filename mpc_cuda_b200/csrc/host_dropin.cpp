@@ -13,6 +13,8 @@
  *   mpbh_fma(prec, n, a, b, c, r)
  *   mpbh_cbinop(prec, op, n, a, b, r)    op 0 cmul, 1 cadd, 2 csub
  *   mpbh_cfma(prec, n, a, b, c, r)       cu_cfma
+ *   mpbh_div(prec, n, a, b, r)           cu_fdiv
+ *   mpbh_sqrt(prec, n, a, r)             cu_sqrt
  *   mpbh_axpy_r / mpbh_axpy_c(prec, n, a, x, y, z)
  *   mpbh_from_double / mpbh_to_double(prec, n, ...)
  * Return 0, or -1 for an unsupported precision.
@@ -49,6 +51,21 @@ void fma3(long n, const void *A, const void *B, const void *C, void *R) {
   auto r = (cu_freal<PB> *)R;
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < n; i++) r[i] = cu_fp::cu_ffma<PB>(a[i], b[i], c[i]);
+}
+template <int PB>
+void div2(long n, const void *A, const void *B, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto b = (const cu_freal<PB> *)B;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_fdiv<PB>(a[i], b[i]);
+}
+template <int PB>
+void sqrt1(long n, const void *A, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_sqrt<PB>(a[i]);
 }
 template <int PB>
 void cfma3(long n, const void *A, const void *B, const void *C, void *R) {
@@ -130,6 +147,12 @@ int mpbh_fma(int prec, long n, const void *a, const void *b, const void *c, void
 }
 int mpbh_cbinop(int prec, int op, long n, const void *a, const void *b, void *r) {
   MPBH_DISPATCH(prec, cbinop<PB>(op, n, a, b, r))
+}
+int mpbh_div(int prec, long n, const void *a, const void *b, void *r) {
+  MPBH_DISPATCH(prec, div2<PB>(n, a, b, r))
+}
+int mpbh_sqrt(int prec, long n, const void *a, void *r) {
+  MPBH_DISPATCH(prec, sqrt1<PB>(n, a, r))
 }
 int mpbh_cfma(int prec, long n, const void *a, const void *b, const void *c, void *r) {
   MPBH_DISPATCH(prec, cfma3<PB>(n, a, b, c, r))

@@ -54,6 +54,8 @@ def lib():
         for name in ("orc_mul", "orc_add", "orc_sub", "orc_cmul", "orc_cadd", "orc_csub",
                      "mp_mul", "mp_add", "mp_sub", "mp_cmul", "mp_cadd", "mp_csub"):
             getattr(L, name).argtypes = [it, lg, vp, vp, vp]
+        L.mp_div.argtypes = [it, lg, vp, vp, vp]
+        L.mp_sqrt.argtypes = [it, lg, vp, vp]
         for name in ("orc_fma", "mp_fma", "mp_cfma", "mp_cfma_dot"):
             getattr(L, name).argtypes = [it, lg, vp, vp, vp, vp]
         for name in ("orc_axpy_r", "orc_axpy_c", "mp_axpy_r", "mp_axpy_c"):
@@ -148,6 +150,28 @@ def binop(kind: str, prec: int, A: np.ndarray, B: np.ndarray, impl: str = "orc")
             raise ValueError(f"reference host build has no PB={prec}")
     else:
         getattr(lib(), f"{impl}_{kind}")(prec, A.shape[0], _p(A), _p(B), _p(R))
+    return R
+
+
+def from_double(prec: int, d) -> np.ndarray:
+    """Exact conversion of doubles to AoS elements (the restatement's from_double)."""
+    d = np.ascontiguousarray(d, dtype=np.float64)
+    R = empty(prec, d.shape[0])
+    lib().orc_from_double(prec, d.shape[0], _p(d), _p(R))
+    return R
+
+
+def div(prec: int, A, B) -> np.ndarray:
+    """round(a / b) by the system MPFR (mpfr_div, RNDN)."""
+    R = empty(prec, A.shape[0])
+    lib().mp_div(prec, A.shape[0], _p(A), _p(B), _p(R))
+    return R
+
+
+def sqrt(prec: int, A) -> np.ndarray:
+    """round(sqrt(a)) by the system MPFR (mpfr_sqrt, RNDN)."""
+    R = empty(prec, A.shape[0])
+    lib().mp_sqrt(prec, A.shape[0], _p(A), _p(R))
     return R
 
 

@@ -957,6 +957,33 @@ void mp_sub(int P, long n, const void *A, const void *B, void *R) {
     finish_out(P, at(R, es, i), r, 0);
   }
 }
+/* correctly rounded division and square root via the system MPFR (checker
+ * for the engine's div / sqrt; the reference's cu_fdiv / cu_sqrt are
+ * faithful only, cu_fmath.cuh:1-14, so MPFR is the specification) */
+void mp_div(int P, long n, const void *A, const void *B, void *R) {
+  size_t es = esz_of(P);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    shim_mpfr_t a, b, r;
+    as_mpfr(P, a, cat(A, es, i));
+    as_mpfr(P, b, cat(B, es, i));
+    bind_out(P, r, at(R, es, i));
+    mpfr_div(r, a, b, SHIM_RNDN);
+    finish_out(P, at(R, es, i), r, 0);
+  }
+}
+void mp_sqrt(int P, long n, const void *A, void *R) {
+  size_t es = esz_of(P);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    shim_mpfr_t a, r;
+    as_mpfr(P, a, cat(A, es, i));
+    bind_out(P, r, at(R, es, i));
+    mpfr_sqrt(r, a, SHIM_RNDN);
+    finish_out(P, at(R, es, i), r, 0);
+  }
+}
+
 void mp_fma(int P, long n, const void *A, const void *B, const void *C, void *R) {
   size_t es = esz_of(P);
 #pragma omp parallel for schedule(static)

@@ -65,6 +65,8 @@ int mpfr_signbit(const shim_mpfr_struct *);
 int mpfr_mul(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *, shim_rnd_t);
 int mpfr_add(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *, shim_rnd_t);
 int mpfr_sub(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_div(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_sqrt(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
 int mpfr_fma(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *,
              const shim_mpfr_struct *, shim_rnd_t);
 int mpfr_fmms(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *,

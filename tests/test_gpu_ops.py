@@ -89,6 +89,25 @@ def test_cmul_cancellation(orc, mpb, prec):
 
 
 @pytest.mark.parametrize("prec", PRECS)
+def test_div_sqrt(orc, mpb, prec):
+    """mpb_div_r / mpb_sqrt_r (the drop-in cu_fdiv / cu_sqrt): one rounding,
+    bit-exact with mpfr_div / mpfr_sqrt, on wide-spread pairs and exact cases."""
+    from test_host_dropin import div_sqrt_cases
+
+    A, B, S = div_sqrt_cases(orc, prec, 20000 if prec <= 1024 else 4000, 0xD5 + prec)
+    M = A.shape[0]
+    r = mpb.empty(prec, M)
+    mpb.div(prec, M, dvec(prec, A), dvec(prec, B), r)
+    bad, first = orc.mismatches(prec, hvec(prec, r, M), orc.div(prec, A, B))
+    assert bad == 0, f"div PB={prec}: {bad} mismatches, first at {first}"
+    M = S.shape[0]
+    r = mpb.empty(prec, M)
+    mpb.sqrt(prec, M, dvec(prec, S), r)
+    bad, first = orc.mismatches(prec, hvec(prec, r, M), orc.sqrt(prec, S))
+    assert bad == 0, f"sqrt PB={prec}: {bad} mismatches, first at {first}"
+
+
+@pytest.mark.parametrize("prec", PRECS)
 def test_binops_complex(orc, mpb, prec):
     M = 30000 if prec <= 1024 else 6000
     A, B = orc.gen_pairs(prec, M, 0xC0DE + prec, cplx=True)

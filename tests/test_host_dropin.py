@@ -134,6 +134,53 @@ def test_cmul_cancellation_uses_exact_products(orc, mpb, prec):
     assert bad == 0, f"PB={prec}: {bad} mismatches, first at {first}"
 
 
+def div_sqrt_cases(orc, prec, M, seed):
+    """(A, B, S) AoS operands for division (A / B) and square root (S):
+    the reference generator's wide-spread pairs, plus exact and structured
+    cases -- a / a, division by powers of two, small integers (1/3, 2/3, ...:
+    repeating patterns), perfect squares k^2 and small non-squares."""
+    A, B = orc.gen_pairs(prec, M, seed)
+    ints = np.arange(1, 65, dtype=np.float64)
+    small = orc.from_double(prec, np.concatenate([ints, ints]))
+    three = orc.from_double(prec, np.concatenate([np.full(64, 3.0), 2.0 ** np.arange(-32, 32)]))
+    A = np.concatenate([A, A[:64], small])
+    B = np.concatenate([B, A[:64].copy(), three])
+    squares = orc.from_double(prec, np.concatenate([ints ** 2, ints, [0.0]]))
+    S = A.copy()
+    S[:, 0:4] = np.array([1], np.int32).view(np.uint8)  # |a|
+    S = np.concatenate([S, squares])
+    return A, B, S
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_div_sqrt_correctly_rounded(orc, mpb, prec):
+    """cu_fdiv / cu_sqrt round the exact quotient / root once (mpfr_div /
+    mpfr_sqrt), unlike the reference's faithful Newton versions."""
+    H = mpb.host_lib()
+    A, B, S = div_sqrt_cases(orc, prec, 3000 if prec <= 1056 else 800, 0xD1 + prec)
+    R = orc.empty(prec, A.shape[0])
+    assert H.mpbh_div(prec, A.shape[0], _p(A), _p(B), _p(R)) == 0
+    bad, first = orc.mismatches(prec, R, orc.div(prec, A, B))
+    assert bad == 0, f"div PB={prec}: {bad} mismatches, first at {first}"
+    R = orc.empty(prec, S.shape[0])
+    assert H.mpbh_sqrt(prec, S.shape[0], _p(S), _p(R)) == 0
+    bad, first = orc.mismatches(prec, R, orc.sqrt(prec, S))
+    assert bad == 0, f"sqrt PB={prec}: {bad} mismatches, first at {first}"
+
+
+@pytest.mark.parametrize("prec", (64, 160, 512))
+def test_div_by_zero_and_sqrt_of_negative_give_zero(orc, mpb, prec):
+    """The format has no infinities or NaN: a / 0 and sqrt(-a) are 0."""
+    H = mpb.host_lib()
+    A = orc.from_double(prec, np.array([1.5, -2.0, 0.0]))
+    Z = orc.from_double(prec, np.zeros(3))
+    R = orc.empty(prec, 3)
+    assert H.mpbh_div(prec, 3, _p(A), _p(Z), _p(R)) == 0
+    assert orc.mismatches(prec, R, Z)[0] == 0
+    assert H.mpbh_sqrt(prec, 1, _p(A[1:2].copy()), _p(R)) == 0
+    assert orc.mismatches(prec, R[:1], Z[:1])[0] == 0
+
+
 def _negate_complex(orc, prec, Z):
     """-Z for complex AoS elements (flip both components' sign words)."""
     es = orc.elem_bytes(prec)
