@@ -2,7 +2,7 @@
 """bench.py -- throughput of the mpb engine on its benchmark workloads.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpb|reference]
-                    [--workload gemm_r512|gemm_c256|gemv_batch|axpy_c1024|axpy_r256]
+                    [--workload gemm_r512|gemm_c256|gemv_batch|axpy_c1024|axpy_r256|div_r512|sqrt_r512]
 
 One JSON line on stdout (rank 0).  A step is one pass of the hot path over
 one batch of synthetic operands already resident in HBM; K steps are timed
@@ -33,6 +33,8 @@ import subprocess
 import sys
 import tempfile
 import time
+
+import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -589,7 +591,97 @@ class GemvBatchWorkload:
                 "l2": "operand pools 7.9 GB of tiles > L2"}
 
 
+class DivSqrtWorkload(AxpyWorkload):
+    """z = round(x / y) or z = round(sqrt(x)) over n elements at precision
+    prec, correctly rounded (mpfr_div / mpfr_sqrt); the reference's CPU
+    baseline is its own faithful cu_fdiv / cu_sqrt built for the host."""
+
+    def __init__(self, name, op, prec, n, seed):
+        super().__init__(name, False, prec, n, seed)
+        self.op = op
+        self.metric = f"correctly rounded {'divisions' if op == 'div' else 'square roots'}/s at PB={prec}"
+        self.unit = "mp-div/s" if op == "div" else "mp-sqrt/s"
+        self.desc = (f"real {'division z=x/y' if op == 'div' else 'square root z=sqrt(x)'}, cu_freal<{prec}>, "
+                     f"RNDN (one rounding), n=2^{n.bit_length() - 1}, full random significands, exponents in "
+                     "[-40, 40]")
+
+    @property
+    def default_steps(self):
+        return 400 if self.op == "div" else 100
+
+    def make_host(self, rank):
+        from mpc_cuda_b200 import layout, synth
+
+        rng = np.random.default_rng(self.seed + 1000 * rank)
+        x = synth.random_elems(rng, self.prec, self.n, -40, 40)
+        y = synth.random_elems(rng, self.prec, self.n, -40, 40)
+        if self.op == "sqrt":
+            x = (x[0], x[1] & np.uint32(0xFFFFFFFE))  # positive
+        a = synth.from_doubles(self.prec, np.array([1.0]))
+        return layout.aos_from_parts(self.prec, *a), layout.aos_from_parts(self.prec, *x), \
+            layout.aos_from_parts(self.prec, *y)
+
+    def step(self, i, stream):
+        x, y, z = self.sets[i % self.nsets]
+        if self.op == "div":
+            self.M.div(self.prec, self.n, x, y, z, stream=stream)
+        else:
+            self.M.sqrt(self.prec, self.n, x, z, stream=stream)
+
+    def e2e_h2d(self, s):
+        self.dx_aos[s].copy_(self.hx, non_blocking=True)
+        if self.op == "div":
+            self.dy_aos[s].copy_(self.hy, non_blocking=True)
+
+    def e2e_bytes(self):
+        return (2 if self.op == "div" else 1) * self.host[1].size, self.host[1].size
+
+    @property
+    def e2e_launches_per_step(self):
+        return 4 if self.op == "div" else 3
+
+    def e2e_compute(self, s, stream):
+        M = self.M
+        M.pack_aos(self.prec, self.n, self.dx_aos[s], self.ex, stream=stream)
+        if self.op == "div":
+            M.pack_aos(self.prec, self.n, self.dy_aos[s], self.ey, stream=stream)
+            M.div(self.prec, self.n, self.ex, self.ey, self.ez, stream=stream)
+        else:
+            M.sqrt(self.prec, self.n, self.ex, self.ez, stream=stream)
+        M.unpack_aos(self.prec, self.n, self.ez, self.dz_aos[s], stream=stream)
+
+    def roofline(self, kernel_s, peaks, imad_ops_s):
+        N = self.prec // 32
+        # multiply-adds (lo + hi) of one long division: (N+2) quotient limbs x N;
+        # the square root runs about log2(32(N+1)/50) + 2 such divisions of
+        # (2N+3) by (N+1) limbs -- an estimate, the iteration count varies
+        per = 2 * N * (N + 2) if self.op == "div" else \
+            int(2 * (N + 1) * (N + 2) * (np.log2(32 * (N + 1) / 50.0) + 2))
+        imad = per * self.n / kernel_s
+        return {"bound": "imad", "achieved": round(imad / 1e9, 1),
+                "peak": round(imad_ops_s / 1e9, 1) if imad_ops_s else None, "unit": "Gop/s",
+                "frac": round(imad / imad_ops_s, 4) if imad_ops_s else None, "ops_per_unit": per,
+                "peak_source": "libmpb_probe.so mad.lo/mad.hi throughput, measured in this run", "traffic": None}
+
+    def cpu_run(self, impl, count):
+        import oracle as O
+
+        _, X, Y = self.host
+        if self.op == "div":
+            O.div(self.prec, X[:count], Y[:count], impl="ref" if impl == "ref" else "mp")
+        else:
+            O.sqrt(self.prec, X[:count], impl="ref" if impl == "ref" else "mp")
+        return count
+
+    def config(self):
+        return {"workload": self.desc, "prec": self.prec, "n": self.n,
+                "units": "one correctly rounded division" if self.op == "div" else "one correctly rounded square root",
+                "l2": f"{self.nsets} rotating input sets > L2"}
+
+
 WORKLOADS = {
+    "div_r512": lambda: DivSqrtWorkload("div_r512", "div", 512, 1 << 20, 0x5EED6),
+    "sqrt_r512": lambda: DivSqrtWorkload("sqrt_r512", "sqrt", 512, 1 << 20, 0x5EED7),
     "gemv_batch": lambda: GemvBatchWorkload("gemv_batch", 4096, 0x5EED4),
     "axpy_c1024": lambda: AxpyWorkload("axpy_c1024", True, 1024, 1 << 18, 0x5EED2),
     "axpy_r256": lambda: AxpyWorkload("axpy_r256", False, 256, 1 << 20, 0x5EED1),
@@ -621,9 +713,9 @@ def cpu_baseline(wl, seconds=10.0):
         el = time.perf_counter() - t0
         if el >= seconds or passes >= 1000:
             break
-    src = ("reference headers include/mpc_cuda/cu_freal.cuh + cu_fcomplex.cuh built for the host "
+    src = ("reference headers include/mpc_cuda/cu_freal.cuh, cu_fcomplex.cuh, cu_fmath.cuh built for the host "
            "(oracle/_ref), OpenMP" if kind == "reference" else "oracle C restatement, OpenMP")
-    return {"value": done / el, "unit": "mp-FMA/s", "cores": O.num_threads(), "kind": kind,
+    return {"value": done / el, "unit": getattr(wl, "unit", "mp-FMA/s"), "cores": O.num_threads(), "kind": kind,
             "sample": f"{passes} pass(es) over {target} of {n_total} units of the same workload, "
                       f"{el:.1f} s; {src}"}
 
@@ -651,13 +743,14 @@ def run_reference(args):
     per_step = done // args.steps
     value = done / dt
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "mp-FMA/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": getattr(wl, "metric", METRIC), "value": value,
+        "unit": getattr(wl, "unit", "mp-FMA/s"), "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic", "config": wl.config(),
-        "cpu_baseline": {"value": value, "unit": "mp-FMA/s", "cores": O.num_threads(), "kind": kind,
+        "cpu_baseline": {"value": value, "unit": getattr(wl, "unit", "mp-FMA/s"), "cores": O.num_threads(), "kind": kind,
                          "sample": f"{per_step} of {wl.units()} units per step"},
-        "e2e": {"value": value, "unit": "mp-FMA/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": value, "unit": getattr(wl, "unit", "mp-FMA/s"), "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -805,14 +898,15 @@ def run_gpu(args):
         cpu = cpu_baseline(wl) if world == 1 and not args.no_cpu else None
         h2d, d2h = wl.e2e_bytes()
         line = {
-            "metric": METRIC, "value": units / (ms_max / 1e3), "unit": "mp-FMA/s", "n_gpus": world,
+            "metric": getattr(wl, "metric", METRIC), "value": units / (ms_max / 1e3),
+            "unit": getattr(wl, "unit", "mp-FMA/s"), "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic", "config": {**wl.config(), "parallelism": f"{world} independent shard(s), "
                                                                           "no collective"},
             "roofline": roof, "cpu_baseline": cpu,
             "e2e": None if ms_e2e is None else {
-                "value": units / (ms_e2e / 1e3), "unit": "mp-FMA/s", "h2d_bytes_per_step": h2d,
+                "value": units / (ms_e2e / 1e3), "unit": getattr(wl, "unit", "mp-FMA/s"), "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps,
                 "path": "pinned host AoS -> H2D -> mpb_pack_aos -> kernel -> mpb_unpack_aos -> D2H, "
                         "double-buffered: H2D, compute and D2H of consecutive steps overlap"},

@@ -105,6 +105,8 @@ def ref():
             getattr(R, name).argtypes = [it, lg, lg, vp, lg, vp, vp, vp]
         for name in ("ref_gemm_r", "ref_gemm_c"):
             getattr(R, name).argtypes = [it, lg, lg, lg, vp, lg, vp, lg, vp, lg, lg, lg]
+        R.ref_div.argtypes = [it, lg, vp, vp, vp]
+        R.ref_sqrt.argtypes = [it, lg, vp, vp]
         R.ref_from_double.argtypes = [it, lg, vp, vp]
         R.ref_to_double.argtypes = [it, lg, vp, vp]
         R.ref_elem_bytes.argtypes = [it]
@@ -161,17 +163,20 @@ def from_double(prec: int, d) -> np.ndarray:
     return R
 
 
-def div(prec: int, A, B) -> np.ndarray:
-    """round(a / b) by the system MPFR (mpfr_div, RNDN)."""
+def div(prec: int, A, B, impl: str = "mp") -> np.ndarray:
+    """a / b: 'mp' = round(a / b) by the system MPFR (mpfr_div, RNDN); 'ref' =
+    the reference's own faithful cu_fdiv built for the host."""
     R = empty(prec, A.shape[0])
-    lib().mp_div(prec, A.shape[0], _p(A), _p(B), _p(R))
+    f = ref().ref_div if impl == "ref" else lib().mp_div
+    f(prec, A.shape[0], _p(A), _p(B), _p(R))
     return R
 
 
-def sqrt(prec: int, A) -> np.ndarray:
-    """round(sqrt(a)) by the system MPFR (mpfr_sqrt, RNDN)."""
+def sqrt(prec: int, A, impl: str = "mp") -> np.ndarray:
+    """sqrt(a): 'mp' = mpfr_sqrt (RNDN); 'ref' = the reference's cu_sqrt."""
     R = empty(prec, A.shape[0])
-    lib().mp_sqrt(prec, A.shape[0], _p(A), _p(R))
+    f = ref().ref_sqrt if impl == "ref" else lib().mp_sqrt
+    f(prec, A.shape[0], _p(A), _p(R))
     return R
 
 

@@ -17,6 +17,7 @@
 #include <cstdint>
 #include <cstring>
 #include "mpc_cuda/cu_fcomplex.cuh"
+#include "mpc_cuda/cu_fmath.cuh"
 
 using cu_fp::cu_fcomplex;
 using cu_fp::cu_freal;
@@ -30,6 +31,24 @@ void t_mul(long n, const void *A, const void *B, void *R) {
   auto r = (cu_freal<PB> *)R;
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < n; i++) r[i] = cu_fp::cu_fmul<PB>(a[i], b[i]);
+}
+/* the reference's division and square root (cu_fmath.cuh:67-75, 92-100:
+ * Newton iteration at PB + CU_FGUARD bits, faithful) -- the CPU baseline of
+ * the engine's correctly rounded mpb_div_r / mpb_sqrt_r */
+template <int PB>
+void t_div(long n, const void *A, const void *B, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto b = (const cu_freal<PB> *)B;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_fdiv<PB>(a[i], b[i]);
+}
+template <int PB>
+void t_sqrt(long n, const void *A, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_sqrt<PB>(a[i]);
 }
 template <int PB>
 void t_add(long n, const void *A, const void *B, void *R) {
@@ -198,6 +217,8 @@ extern "C" {
 int ref_elem_bytes(int P) { REF_DISPATCH(P, return (int)sizeof(cu_freal<PB>)) }
 int ref_mul(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_mul<PB>(n, A, B, R)) }
 int ref_add(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_add<PB>(n, A, B, R)) }
+int ref_div(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_div<PB>(n, A, B, R)) }
+int ref_sqrt(int P, long n, const void *A, void *R) { REF_DISPATCH(P, t_sqrt<PB>(n, A, R)) }
 int ref_sub(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_sub<PB>(n, A, B, R)) }
 int ref_cmul(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_cmul<PB>(n, A, B, R)) }
 int ref_cadd(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_cadd<PB>(n, A, B, R)) }
