@@ -607,7 +607,7 @@ class DivSqrtWorkload(AxpyWorkload):
 
     @property
     def default_steps(self):
-        return 400 if self.op == "div" else 100
+        return 8000 if self.op == "div" else 1300  # about 1 s of GPU time: long enough for clock sampling
 
     def make_host(self, rank):
         from mpc_cuda_b200 import layout, synth

@@ -118,6 +118,21 @@ MPB_HD uint32_t madchi(uint32_t a, uint32_t b, uint32_t c, uint32_t &) {
   asm volatile("madc.hi.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
   return d;
 }
+MPB_HD uint32_t sub_cc(uint32_t a, uint32_t b, uint32_t &) { /* CF = borrow */
+  uint32_t d;
+  asm volatile("sub.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+MPB_HD uint32_t subc_cc(uint32_t a, uint32_t b, uint32_t &) {
+  uint32_t d;
+  asm volatile("subc.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+MPB_HD uint32_t subc(uint32_t a, uint32_t b, uint32_t &) {
+  uint32_t d;
+  asm volatile("subc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
 MPB_HD uint32_t mulhi(uint32_t a, uint32_t b) { return __umulhi(a, b); }
 MPB_HD uint32_t fshl(uint32_t lo, uint32_t hi, uint32_t s) { return __funnelshift_l(lo, hi, s); }
 MPB_HD uint32_t fshr(uint32_t lo, uint32_t hi, uint32_t s) { return __funnelshift_r(lo, hi, s); }
@@ -161,6 +176,16 @@ MPB_HD uint32_t madchi_cc(uint32_t a, uint32_t b, uint32_t c, uint32_t &cf) {
 MPB_HD uint32_t madchi(uint32_t a, uint32_t b, uint32_t c, uint32_t &cf) {
   return (uint32_t)(((uint64_t)a * b) >> 32) + c + cf;
 }
+MPB_HD uint32_t sub_cc(uint32_t a, uint32_t b, uint32_t &cf) {
+  cf = a < b ? 1u : 0u;
+  return a - b;
+}
+MPB_HD uint32_t subc_cc(uint32_t a, uint32_t b, uint32_t &cf) {
+  const uint64_t t = (uint64_t)a - b - cf;
+  cf = (uint32_t)(t >> 63);
+  return (uint32_t)t;
+}
+MPB_HD uint32_t subc(uint32_t a, uint32_t b, uint32_t &cf) { return a - b - cf; }
 MPB_HD uint32_t mulhi(uint32_t a, uint32_t b) { return (uint32_t)(((uint64_t)a * b) >> 32); }
 MPB_HD uint32_t fshl(uint32_t lo, uint32_t hi, uint32_t s) {
   return (uint32_t)((((uint64_t)hi << 32) | lo) << (s & 31) >> 32);
@@ -790,48 +815,73 @@ MPB_HD void cfma(fval<N> &rr, fval<N> &ri, const fval<N> &ar, const fval<N> &ai,
  * index known at compile time: q[0 .. NU-NV) = floor(U / V) and u[0 .. NV)
  * becomes U mod V.  V must be normalised (top bit of v[NV-1] set) and
  * U < V * 2^(32 (NU - NV)).  Each quotient limb is estimated from the top two
- * remainder limbs and the top divisor limb, corrected with the second
- * divisor limb (at most twice), and fixed by one add-back when the
- * multiply-subtract goes negative. */
+ * remainder limbs and the top divisor limb d by the 2-by-1 division of
+ * Moeller and Granlund ("Improved division by invariant integers", IEEE
+ * Trans. Computers 2011) with the reciprocal floor((2^64 - 1) / d) - 2^32
+ * computed once, corrected with the second divisor limb (at most twice,
+ * Knuth's test), and fixed by one add-back when the multiply-subtract -- a
+ * carry chain over the limb product and a borrow chain over the remainder
+ * -- goes negative. */
 template <int NU, int NV>
 MPB_HD void divmod_limbs(uint32_t *q, uint32_t *u, const uint32_t *v) {
-  const uint64_t v1 = v[NV - 1];
+  const uint32_t d = v[NV - 1];
   const uint64_t v2 = NV >= 2 ? v[NV - 2 >= 0 ? NV - 2 : 0] : 0u;
+  const uint32_t rcp = (uint32_t)(0xffffffffffffffffull / d - (1ull << 32));
   MPB_UNROLL
   for (int j = NU - NV - 1; j >= 0; --j) {
-    const uint64_t num = ((uint64_t)u[j + NV] << 32) | u[j + NV - 1];
-    uint64_t qh = num / v1, rh = num - qh * v1;
+    const uint32_t u1 = u[j + NV], u0 = u[j + NV - 1];
+    uint64_t qh, rh;
+    if (u1 >= d) { /* (u1 = d): the estimate is 2^32 - 1 */
+      qh = 0xffffffffull;
+      rh = (uint64_t)u0 + d;
+    } else { /* 2-by-1 division with the reciprocal */
+      const uint64_t qq = (uint64_t)rcp * u1 + (((uint64_t)u1 << 32) | u0);
+      uint32_t q1 = (uint32_t)(qq >> 32) + 1u;
+      const uint32_t q0 = (uint32_t)qq;
+      uint32_t r = u0 - q1 * d;
+      if (r > q0) {
+        --q1;
+        r += d;
+      }
+      if (r >= d) {
+        ++q1;
+        r -= d;
+      }
+      qh = q1;
+      rh = r;
+    }
     const uint64_t u3 = (j + NV - 2 >= 0) ? u[j + NV - 2 >= 0 ? j + NV - 2 : 0] : 0u;
     MPB_UNROLL
     for (int c = 0; c < 2; ++c) {
-      if (rh < (1ull << 32) && (qh >= (1ull << 32) || qh * v2 > ((rh << 32) | u3))) {
+      if (rh < (1ull << 32) && qh * v2 > ((rh << 32) | u3)) {
         --qh;
-        rh += v1;
+        rh += d;
       }
     }
-    /* u[j .. j+NV] -= qh * v */
-    uint64_t carry = 0;
-    uint32_t borrow = 0;
-    MPB_UNROLL
-    for (int i = 0; i < NV; ++i) {
-      const uint64_t p = qh * v[i] + carry;
-      carry = p >> 32;
-      const uint64_t t = (uint64_t)u[j + i] - (uint32_t)p - borrow;
-      u[j + i] = (uint32_t)t;
-      borrow = (uint32_t)(t >> 63);
-    }
-    const uint64_t top = (uint64_t)u[j + NV] - carry - borrow;
-    u[j + NV] = (uint32_t)top;
-    if (top >> 63) { /* estimate one too large: add v back */
-      --qh;
-      uint64_t c = 0;
+    const uint32_t qd = (uint32_t)qh;
+    /* P = qd * v (NV + 1 limbs), then u[j .. j+NV] -= P */
+    uint32_t pl[NV + 1];
+    {
+      uint32_t cf = 0;
+      pl[0] = qd * v[0];
       MPB_UNROLL
-      for (int i = 0; i < NV; ++i) {
-        const uint64_t t = (uint64_t)u[j + i] + v[i] + c;
-        u[j + i] = (uint32_t)t;
-        c = t >> 32;
-      }
-      u[j + NV] += (uint32_t)c;
+      for (int i = 1; i < NV; ++i) pl[i] = (i == 1) ? add_cc(qd * v[i], mulhi(qd, v[i - 1]), cf)
+                                                    : addc_cc(qd * v[i], mulhi(qd, v[i - 1]), cf);
+      pl[NV] = (NV == 1) ? mulhi(qd, v[NV - 1]) : addc(mulhi(qd, v[NV - 1]), 0u, cf);
+    }
+    uint32_t bf = 0;
+    u[j] = sub_cc(u[j], pl[0], bf);
+    MPB_UNROLL
+    for (int i = 1; i < NV; ++i) u[j + i] = subc_cc(u[j + i], pl[i], bf);
+    u[j + NV] = subc_cc(u[j + NV], pl[NV], bf);
+    const uint32_t neg = subc(0u, 0u, bf); /* all ones when the result went negative */
+    if (neg) { /* estimate one too large: add v back */
+      qh = qd - 1u;
+      uint32_t cf = 0;
+      u[j] = add_cc(u[j], v[0], cf);
+      MPB_UNROLL
+      for (int i = 1; i < NV; ++i) u[j + i] = addc_cc(u[j + i], v[i], cf);
+      u[j + NV] = addc(u[j + NV], 0u, cf);
     }
     q[j] = (uint32_t)qh;
   }
