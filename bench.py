@@ -2,7 +2,8 @@
 """bench.py -- throughput of the mpb engine on its benchmark workloads.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpb|reference]
-                    [--workload gemm_r512|gemm_c256|gemv_batch|axpy_c1024|axpy_r256|div_r512|sqrt_r512]
+                    [--workload gemm_r512|gemm_c256|gemv_batch|axpy_c1024|axpy_r256|
+                                div_r512|sqrt_r512|exp_r512|log_r512]
 
 One JSON line on stdout (rank 0).  A step is one pass of the hot path over
 one batch of synthetic operands already resident in HBM; K steps are timed
@@ -592,30 +593,35 @@ class GemvBatchWorkload:
 
 
 class DivSqrtWorkload(AxpyWorkload):
-    """z = round(x / y) or z = round(sqrt(x)) over n elements at precision
-    prec, correctly rounded (mpfr_div / mpfr_sqrt); the reference's CPU
-    baseline is its own faithful cu_fdiv / cu_sqrt built for the host."""
+    """z = x / y, sqrt(x) (correctly rounded: mpfr_div / mpfr_sqrt), exp(x) or
+    log(x) (faithful, the reference's contract) over n elements at precision
+    prec; the CPU baseline is the reference's own cu_fdiv / cu_sqrt / cu_exp /
+    cu_log built for the host."""
+
+    NAMES = {"div": ("correctly rounded divisions", "mp-div/s", "division z=x/y, RNDN (one rounding)"),
+             "sqrt": ("correctly rounded square roots", "mp-sqrt/s", "square root z=sqrt(x), RNDN (one rounding)"),
+             "exp": ("faithful exponentials", "mp-exp/s", "exponential z=exp(x), faithful (x in (-8, 8))"),
+             "log": ("faithful logarithms", "mp-log/s", "logarithm z=log(x), faithful (x > 0)")}
 
     def __init__(self, name, op, prec, n, seed):
         super().__init__(name, False, prec, n, seed)
         self.op = op
-        self.metric = f"correctly rounded {'divisions' if op == 'div' else 'square roots'}/s at PB={prec}"
-        self.unit = "mp-div/s" if op == "div" else "mp-sqrt/s"
-        self.desc = (f"real {'division z=x/y' if op == 'div' else 'square root z=sqrt(x)'}, cu_freal<{prec}>, "
-                     f"RNDN (one rounding), n=2^{n.bit_length() - 1}, full random significands, exponents in "
-                     "[-40, 40]")
+        what, self.unit, desc = self.NAMES[op]
+        self.metric = f"{what}/s at PB={prec}"
+        self.desc = (f"real {desc}, cu_freal<{prec}>, n=2^{n.bit_length() - 1}, full random significands")
 
     @property
-    def default_steps(self):
-        return 8000 if self.op == "div" else 1300  # about 1 s of GPU time: long enough for clock sampling
+    def default_steps(self):  # about 1 s of GPU time: long enough for clock sampling
+        return {"div": 8000, "sqrt": 1300, "exp": 100, "log": 30}[self.op]
 
     def make_host(self, rank):
         from mpc_cuda_b200 import layout, synth
 
         rng = np.random.default_rng(self.seed + 1000 * rank)
-        x = synth.random_elems(rng, self.prec, self.n, -40, 40)
-        y = synth.random_elems(rng, self.prec, self.n, -40, 40)
-        if self.op == "sqrt":
+        lo, hi = {"div": (-40, 40), "sqrt": (-40, 40), "exp": (-3, 3), "log": (-20, 20)}[self.op]
+        x = synth.random_elems(rng, self.prec, self.n, lo, hi)
+        y = synth.random_elems(rng, self.prec, self.n, lo, hi)
+        if self.op in ("sqrt", "log"):
             x = (x[0], x[1] & np.uint32(0xFFFFFFFE))  # positive
         a = synth.from_doubles(self.prec, np.array([1.0]))
         return layout.aos_from_parts(self.prec, *a), layout.aos_from_parts(self.prec, *x), \
@@ -626,7 +632,7 @@ class DivSqrtWorkload(AxpyWorkload):
         if self.op == "div":
             self.M.div(self.prec, self.n, x, y, z, stream=stream)
         else:
-            self.M.sqrt(self.prec, self.n, x, z, stream=stream)
+            getattr(self.M, self.op)(self.prec, self.n, x, z, stream=stream)
 
     def e2e_h2d(self, s):
         self.dx_aos[s].copy_(self.hx, non_blocking=True)
@@ -647,16 +653,24 @@ class DivSqrtWorkload(AxpyWorkload):
             M.pack_aos(self.prec, self.n, self.dy_aos[s], self.ey, stream=stream)
             M.div(self.prec, self.n, self.ex, self.ey, self.ez, stream=stream)
         else:
-            M.sqrt(self.prec, self.n, self.ex, self.ez, stream=stream)
+            getattr(M, self.op)(self.prec, self.n, self.ex, self.ez, stream=stream)
         M.unpack_aos(self.prec, self.n, self.ez, self.dz_aos[s], stream=stream)
 
     def roofline(self, kernel_s, peaks, imad_ops_s):
         N = self.prec // 32
-        # multiply-adds (lo + hi) of one long division: (N+2) quotient limbs x N;
-        # the square root runs about log2(32(N+1)/50) + 2 such divisions of
-        # (2N+3) by (N+1) limbs -- an estimate, the iteration count varies
-        per = 2 * N * (N + 2) if self.op == "div" else \
-            int(2 * (N + 1) * (N + 2) * (np.log2(32 * (N + 1) / 50.0) + 2))
+        NW = N + 4  # exp / log working precision
+        mulw, divw = rounded_product_imads(NW), 2 * NW * (NW + 2)
+        terms = 32 * NW // 17 + 3
+        exp_ops = terms * (mulw + divw) + 17 * mulw
+        # multiply-adds (lo + hi) per element: a long division is (N+2) quotient
+        # limbs x N; the square root runs about log2(32(N+1)/50) + 2 divisions of
+        # (2N+3) by (N+1) limbs; exp is the Taylor terms (a product and a division
+        # each) plus 16 squarings at N+4 limbs; log (away from 1) about
+        # log2(32(N+4)/20) Newton steps of one exp -- estimates: counts vary
+        per = {"div": 2 * N * (N + 2),
+               "sqrt": int(2 * (N + 1) * (N + 2) * (np.log2(32 * (N + 1) / 50.0) + 2)),
+               "exp": exp_ops,
+               "log": int((np.log2(32 * NW / 20.0) + 1) * (exp_ops + mulw))}[self.op]
         imad = per * self.n / kernel_s
         return {"bound": "imad", "achieved": round(imad / 1e9, 1),
                 "peak": round(imad_ops_s / 1e9, 1) if imad_ops_s else None, "unit": "Gop/s",
@@ -667,21 +681,25 @@ class DivSqrtWorkload(AxpyWorkload):
         import oracle as O
 
         _, X, Y = self.host
+        kind = "ref" if impl == "ref" else "mp"
         if self.op == "div":
-            O.div(self.prec, X[:count], Y[:count], impl="ref" if impl == "ref" else "mp")
+            O.div(self.prec, X[:count], Y[:count], impl=kind)
         else:
-            O.sqrt(self.prec, X[:count], impl="ref" if impl == "ref" else "mp")
+            getattr(O, self.op)(self.prec, X[:count], impl=kind)
         return count
 
     def config(self):
         return {"workload": self.desc, "prec": self.prec, "n": self.n,
-                "units": "one correctly rounded division" if self.op == "div" else "one correctly rounded square root",
+                "units": "one " + {"div": "correctly rounded division", "sqrt": "correctly rounded square root",
+                                   "exp": "faithful exponential", "log": "faithful logarithm"}[self.op],
                 "l2": f"{self.nsets} rotating input sets > L2"}
 
 
 WORKLOADS = {
     "div_r512": lambda: DivSqrtWorkload("div_r512", "div", 512, 1 << 20, 0x5EED6),
     "sqrt_r512": lambda: DivSqrtWorkload("sqrt_r512", "sqrt", 512, 1 << 20, 0x5EED7),
+    "exp_r512": lambda: DivSqrtWorkload("exp_r512", "exp", 512, 1 << 18, 0x5EED8),
+    "log_r512": lambda: DivSqrtWorkload("log_r512", "log", 512, 1 << 18, 0x5EED9),
     "gemv_batch": lambda: GemvBatchWorkload("gemv_batch", 4096, 0x5EED4),
     "axpy_c1024": lambda: AxpyWorkload("axpy_c1024", True, 1024, 1 << 18, 0x5EED2),
     "axpy_r256": lambda: AxpyWorkload("axpy_r256", False, 256, 1 << 20, 0x5EED1),

@@ -94,6 +94,12 @@ int mpb_fma_r(int prec, size_t n, const void *a, const void *b, const void *c, v
  * format has no infinities or NaN). */
 int mpb_div_r(int prec, size_t n, const void *a, const void *b, void *r, void *stream);
 int mpb_sqrt_r(int prec, size_t n, const void *a, void *r, void *stream);
+/* r[i] = exp(a[i]), r[i] = log(a[i]): faithful (at most 1 ULP from the exact
+ * value), the contract of the reference's cu_exp / cu_log
+ * (include/mpc_cuda/cu_fmath.cuh:197-218); computed at 128 guard bits.  exp
+ * of |a| >= 2^29 (result outside the exponent range) and log of a <= 0 give 0. */
+int mpb_exp_r(int prec, size_t n, const void *a, void *r, void *stream);
+int mpb_log_r(int prec, size_t n, const void *a, void *r, void *stream);
 /* complex r[i] = a[i]*b[i] + c[i], one rounding per component from exact
  * products (mpc_fma; the drop-in cu_cfma; no counterpart in the reference) */
 int mpb_fma_c(int prec, size_t n, const void *a, const void *b, const void *c, void *r, void *stream);

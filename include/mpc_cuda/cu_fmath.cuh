@@ -10,13 +10,16 @@
  * known.  A quotient by zero or the square root of a negative number has no
  * value in this format (no infinities or NaN): the result is 0.
  *
- * The reference's elementary functions (exp, log, trig, ...) are not part of
- * this engine.
+ * cu_exp / cu_log (reference cu_fmath.cuh:197-218) keep the reference's
+ * contract: faithful, within 1 ULP of MPFR (mpb/elem.cuh: 128 guard bits).
+ * The reference's other elementary functions (expm1, log1p, trigonometric,
+ * hyperbolic, pow, cbrt) are not part of this engine.
  */
 #ifndef MPB_DROPIN_CU_FMATH_CUH
 #define MPB_DROPIN_CU_FMATH_CUH
 
 #include "cu_freal.cuh"
+#include "../mpb/elem.cuh"
 
 namespace cu_fp {
 
@@ -36,6 +39,24 @@ __host__ __device__ static inline cu_freal<PB> cu_sqrt(const cu_freal<PB> &x) {
   typename detail::core_of<PB>::type a, r;
   detail::to_core<PB>(a, x);
   mpb::sqrt_(r, a);
+  return detail::from_core<PB>(r);
+}
+
+/* exp(x), faithful (at most 1 ULP; exp of |x| >= 2^29 gives 0) */
+template <int PB>
+__host__ __device__ static inline cu_freal<PB> cu_exp(const cu_freal<PB> &x) {
+  typename detail::core_of<PB>::type a, r;
+  detail::to_core<PB>(a, x);
+  mpb::exp_(r, a);
+  return detail::from_core<PB>(r);
+}
+
+/* log(x), faithful (at most 1 ULP; x <= 0 gives 0) */
+template <int PB>
+__host__ __device__ static inline cu_freal<PB> cu_log(const cu_freal<PB> &x) {
+  typename detail::core_of<PB>::type a, r;
+  detail::to_core<PB>(a, x);
+  mpb::log_(r, a);
   return detail::from_core<PB>(r);
 }
 

@@ -60,6 +60,8 @@ _SIGS = {
     "mpb_fma_c": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
     "mpb_div_r": ([_I, _S, _V, _V, _V, _V], C.c_int),
     "mpb_sqrt_r": ([_I, _S, _V, _V, _V], C.c_int),
+    "mpb_exp_r": ([_I, _S, _V, _V, _V], C.c_int),
+    "mpb_log_r": ([_I, _S, _V, _V, _V], C.c_int),
     "mpb_binop_c": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
     "mpb_axpy_r": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
     "mpb_axpy_c": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
@@ -125,6 +127,8 @@ def host_lib():
         H.mpbh_cfma.argtypes = [_I, _L, _V, _V, _V, _V]
         H.mpbh_div.argtypes = [_I, _L, _V, _V, _V]
         H.mpbh_sqrt.argtypes = [_I, _L, _V, _V]
+        H.mpbh_exp.argtypes = [_I, _L, _V, _V]
+        H.mpbh_log.argtypes = [_I, _L, _V, _V]
         for name in ("mpbh_axpy_r", "mpbh_axpy_c"):
             getattr(H, name).argtypes = [_I, _L, _V, _V, _V, _V]
         H.mpbh_from_double.argtypes = [_I, _L, _V, _V]
@@ -213,6 +217,16 @@ def div(prec, n, a, b, r, stream=None):
 def sqrt(prec, n, a, r, stream=None):
     """r = round(sqrt(a)), one rounding (0 where a < 0)."""
     _call("mpb_sqrt_r", prec, n, _ptr(a), _ptr(r), _stream(stream))
+
+
+def exp(prec, n, a, r, stream=None):
+    """r = exp(a), faithful (0 where |a| >= 2^29)."""
+    _call("mpb_exp_r", prec, n, _ptr(a), _ptr(r), _stream(stream))
+
+
+def log(prec, n, a, r, stream=None):
+    """r = log(a), faithful (0 where a <= 0)."""
+    _call("mpb_log_r", prec, n, _ptr(a), _ptr(r), _stream(stream))
 
 
 def fma(prec, n, a, b, c, r, cplx=False, stream=None):
@@ -336,7 +350,8 @@ class BatchGemv:
 
 __all__ = [
     "SUPPORTED", "MpbError", "aos_bytes", "tile_bytes", "vec_bytes", "build", "lib", "host_lib", "empty",
-    "empty_matrix", "pack_aos", "unpack_aos", "from_double", "to_double", "binop", "fma", "div", "sqrt", "axpy",
+    "empty_matrix", "pack_aos", "unpack_aos", "from_double", "to_double", "binop", "fma", "div", "sqrt", "exp", "log",
+    "axpy",
     "gemv", "gemm",
     "layout", "MPB_OP_MUL", "MPB_OP_ADD", "MPB_OP_SUB", "gemm_exact", "gemm_exact_workspace", "gemm_exact_info",
     "BatchGemv",

@@ -15,6 +15,7 @@
  *   mpbh_cfma(prec, n, a, b, c, r)       cu_cfma
  *   mpbh_div(prec, n, a, b, r)           cu_fdiv
  *   mpbh_sqrt(prec, n, a, r)             cu_sqrt
+ *   mpbh_exp / mpbh_log(prec, n, a, r)   cu_exp / cu_log
  *   mpbh_axpy_r / mpbh_axpy_c(prec, n, a, x, y, z)
  *   mpbh_from_double / mpbh_to_double(prec, n, ...)
  * Return 0, or -1 for an unsupported precision.
@@ -66,6 +67,20 @@ void sqrt1(long n, const void *A, void *R) {
   auto r = (cu_freal<PB> *)R;
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < n; i++) r[i] = cu_fp::cu_sqrt<PB>(a[i]);
+}
+template <int PB>
+void exp1(long n, const void *A, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_exp<PB>(a[i]);
+}
+template <int PB>
+void log1(long n, const void *A, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_log<PB>(a[i]);
 }
 template <int PB>
 void cfma3(long n, const void *A, const void *B, const void *C, void *R) {
@@ -154,6 +169,8 @@ int mpbh_div(int prec, long n, const void *a, const void *b, void *r) {
 int mpbh_sqrt(int prec, long n, const void *a, void *r) {
   MPBH_DISPATCH(prec, sqrt1<PB>(n, a, r))
 }
+int mpbh_exp(int prec, long n, const void *a, void *r) { MPBH_DISPATCH(prec, exp1<PB>(n, a, r)) }
+int mpbh_log(int prec, long n, const void *a, void *r) { MPBH_DISPATCH(prec, log1<PB>(n, a, r)) }
 int mpbh_cfma(int prec, long n, const void *a, const void *b, const void *c, void *r) {
   MPBH_DISPATCH(prec, cfma3<PB>(n, a, b, c, r))
 }

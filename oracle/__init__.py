@@ -56,6 +56,8 @@ def lib():
             getattr(L, name).argtypes = [it, lg, vp, vp, vp]
         L.mp_div.argtypes = [it, lg, vp, vp, vp]
         L.mp_sqrt.argtypes = [it, lg, vp, vp]
+        L.mp_exp.argtypes = [it, it, lg, vp, vp]
+        L.mp_log.argtypes = [it, it, lg, vp, vp]
         for name in ("orc_fma", "mp_fma", "mp_cfma", "mp_cfma_dot"):
             getattr(L, name).argtypes = [it, lg, vp, vp, vp, vp]
         for name in ("orc_axpy_r", "orc_axpy_c", "mp_axpy_r", "mp_axpy_c"):
@@ -107,6 +109,8 @@ def ref():
             getattr(R, name).argtypes = [it, lg, lg, lg, vp, lg, vp, lg, vp, lg, lg, lg]
         R.ref_div.argtypes = [it, lg, vp, vp, vp]
         R.ref_sqrt.argtypes = [it, lg, vp, vp]
+        R.ref_exp.argtypes = [it, lg, vp, vp]
+        R.ref_log.argtypes = [it, lg, vp, vp]
         R.ref_from_double.argtypes = [it, lg, vp, vp]
         R.ref_to_double.argtypes = [it, lg, vp, vp]
         R.ref_elem_bytes.argtypes = [it]
@@ -177,6 +181,29 @@ def sqrt(prec: int, A, impl: str = "mp") -> np.ndarray:
     R = empty(prec, A.shape[0])
     f = ref().ref_sqrt if impl == "ref" else lib().mp_sqrt
     f(prec, A.shape[0], _p(A), _p(R))
+    return R
+
+
+def exp(prec: int, A, out_prec: int | None = None, impl: str = "mp") -> np.ndarray:
+    """exp(a): 'mp' = mpfr_exp rounded at out_prec bits (default prec); 'ref' =
+    the reference's own faithful cu_exp built for the host."""
+    po = out_prec or prec
+    R = empty(po, A.shape[0])
+    if impl == "ref":
+        ref().ref_exp(prec, A.shape[0], _p(A), _p(R))
+    else:
+        lib().mp_exp(prec, po, A.shape[0], _p(A), _p(R))
+    return R
+
+
+def log(prec: int, A, out_prec: int | None = None, impl: str = "mp") -> np.ndarray:
+    """log(a): 'mp' = mpfr_log at out_prec bits; 'ref' = the reference's cu_log."""
+    po = out_prec or prec
+    R = empty(po, A.shape[0])
+    if impl == "ref":
+        ref().ref_log(prec, A.shape[0], _p(A), _p(R))
+    else:
+        lib().mp_log(prec, po, A.shape[0], _p(A), _p(R))
     return R
 
 

@@ -972,6 +972,24 @@ void mp_div(int P, long n, const void *A, const void *B, void *R) {
     finish_out(P, at(R, es, i), r, 0);
   }
 }
+/* mpfr_exp / mpfr_log at precision Pout (the checker for the engine's
+ * faithful exp / log: Pout = 4P measures the error in ULPs) */
+typedef int (*mpfr_un_t)(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+static void mp_un(mpfr_un_t f, int P, int Pout, long n, const void *A, void *R) {
+  size_t es = esz_of(P), eo = esz_of(Pout);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    shim_mpfr_t a, r;
+    as_mpfr(P, a, cat(A, es, i));
+    mpfr_init2(r, Pout);
+    f(r, a, SHIM_RNDN);
+    store_mpfr(Pout, at(R, eo, i), r);
+    mpfr_clear(r);
+  }
+}
+void mp_exp(int P, int Pout, long n, const void *A, void *R) { mp_un(mpfr_exp, P, Pout, n, A, R); }
+void mp_log(int P, int Pout, long n, const void *A, void *R) { mp_un(mpfr_log, P, Pout, n, A, R); }
+
 void mp_sqrt(int P, long n, const void *A, void *R) {
   size_t es = esz_of(P);
 #pragma omp parallel for schedule(static)

@@ -67,6 +67,8 @@ int mpfr_add(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *, 
 int mpfr_sub(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *, shim_rnd_t);
 int mpfr_div(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *, shim_rnd_t);
 int mpfr_sqrt(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_exp(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_log(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
 int mpfr_fma(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *,
              const shim_mpfr_struct *, shim_rnd_t);
 int mpfr_fmms(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *,

@@ -51,6 +51,20 @@ void t_sqrt(long n, const void *A, void *R) {
   for (long i = 0; i < n; i++) r[i] = cu_fp::cu_sqrt<PB>(a[i]);
 }
 template <int PB>
+void t_exp(long n, const void *A, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_exp<PB>(a[i]);
+}
+template <int PB>
+void t_log(long n, const void *A, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_log<PB>(a[i]);
+}
+template <int PB>
 void t_add(long n, const void *A, const void *B, void *R) {
   auto a = (const cu_freal<PB> *)A;
   auto b = (const cu_freal<PB> *)B;
@@ -219,6 +233,8 @@ int ref_mul(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH
 int ref_add(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_add<PB>(n, A, B, R)) }
 int ref_div(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_div<PB>(n, A, B, R)) }
 int ref_sqrt(int P, long n, const void *A, void *R) { REF_DISPATCH(P, t_sqrt<PB>(n, A, R)) }
+int ref_exp(int P, long n, const void *A, void *R) { REF_DISPATCH(P, t_exp<PB>(n, A, R)) }
+int ref_log(int P, long n, const void *A, void *R) { REF_DISPATCH(P, t_log<PB>(n, A, R)) }
 int ref_sub(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_sub<PB>(n, A, B, R)) }
 int ref_cmul(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_cmul<PB>(n, A, B, R)) }
 int ref_cadd(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_cadd<PB>(n, A, B, R)) }

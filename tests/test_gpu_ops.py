@@ -108,6 +108,29 @@ def test_div_sqrt(orc, mpb, prec):
 
 
 @pytest.mark.parametrize("prec", PRECS)
+def test_exp_log(orc, mpb, prec):
+    """mpb_exp_r / mpb_log_r: within 1 ULP of MPFR, and bit-identical to the
+    host build of the same drop-in functions."""
+    import ctypes as C
+
+    from test_host_dropin import exp_log_cases
+
+    H = mpb.host_lib()
+    X, Y = exp_log_cases(orc, prec, 2000 if prec <= 512 else 400, 0xE5 + prec)
+    pref = min(4 * prec, orc.lib().orc_max_prec())
+    for name, f, hf, A, ref in (("exp", mpb.exp, H.mpbh_exp, X, orc.exp), ("log", mpb.log, H.mpbh_log, Y, orc.log)):
+        M = A.shape[0]
+        r = mpb.empty(prec, M)
+        f(prec, M, dvec(prec, A), r)
+        got = hvec(prec, r, M)
+        ulp = orc.ulp_errors(prec, got, pref, ref(prec, A, pref))
+        assert ulp.max() <= 1.0, f"{name} PB={prec}: {ulp.max():.3f} ULP"
+        host = orc.empty(prec, M)
+        hf(prec, M, A.ctypes.data_as(C.c_void_p), host.ctypes.data_as(C.c_void_p))
+        assert orc.mismatches(prec, got, host)[0] == 0, f"{name} PB={prec}: device differs from host build"
+
+
+@pytest.mark.parametrize("prec", PRECS)
 def test_binops_complex(orc, mpb, prec):
     M = 30000 if prec <= 1024 else 6000
     A, B = orc.gen_pairs(prec, M, 0xC0DE + prec, cplx=True)

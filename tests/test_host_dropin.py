@@ -181,6 +181,36 @@ def test_div_by_zero_and_sqrt_of_negative_give_zero(orc, mpb, prec):
     assert orc.mismatches(prec, R[:1], Z[:1])[0] == 0
 
 
+def exp_log_cases(orc, prec, M, seed):
+    """In-range arguments for exp (doubles in [-8, 8] as in the reference's
+    test, plus the wide generator's values below 2^8) and positive ones for
+    log (|wide generator| plus values within 2^-10 of 1)."""
+    A, _ = orc.gen_pairs(prec, M, seed)
+    ea = A[:, 8:16].copy().view(np.int64).ravel()
+    rng = np.random.default_rng(seed)
+    X = np.concatenate([orc.from_double(prec, rng.uniform(-8, 8, M)), A[(ea <= 8) & (ea >= -300)][: M // 2]])
+    Y = A.copy()
+    Y[:, 0:4] = np.array([1], np.int32).view(np.uint8)
+    Y = np.concatenate([Y, orc.from_double(prec, 1 + rng.uniform(-1e-3, 1e-3, 64))])
+    return X, Y
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_exp_log_faithful(orc, mpb, prec):
+    """cu_exp / cu_log: within 1 ULP of MPFR (the reference's contract); with
+    128 guard bits they are in practice correctly rounded, so the results must
+    also equal mpfr_exp / mpfr_log on nearly every argument."""
+    H = mpb.host_lib()
+    X, Y = exp_log_cases(orc, prec, 400 if prec <= 1056 else 100, 0xE1 + prec)
+    pref = min(4 * prec, orc.lib().orc_max_prec())
+    for name, f, A, ref in (("exp", H.mpbh_exp, X, orc.exp), ("log", H.mpbh_log, Y, orc.log)):
+        R = orc.empty(prec, A.shape[0])
+        assert f(prec, A.shape[0], _p(A), _p(R)) == 0
+        ulp = orc.ulp_errors(prec, R, pref, ref(prec, A, pref))
+        assert ulp.max() <= 1.0, f"{name} PB={prec}: {ulp.max():.3f} ULP"
+        assert orc.mismatches(prec, R, ref(prec, A))[0] <= A.shape[0] // 100, name
+
+
 def _negate_complex(orc, prec, Z):
     """-Z for complex AoS elements (flip both components' sign words)."""
     es = orc.elem_bytes(prec)
