@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpb|reference]
                     [--workload gemm_r512|gemm_c256|gemv_batch|axpy_c1024|axpy_r256|
-                                div_r512|sqrt_r512|exp_r512|log_r512]
+                                div_r512|sqrt_r512|exp_r512|log_r512|sin_r512]
 
 One JSON line on stdout (rank 0).  A step is one pass of the hot path over
 one batch of synthetic operands already resident in HBM; K steps are timed
@@ -592,16 +592,41 @@ class GemvBatchWorkload:
                 "l2": "operand pools 7.9 GB of tiles > L2"}
 
 
+def _elem_params(NW):
+    """the series parameters of mpb/elem.cuh at NW limbs (em1_halvings ..
+    odd_terms there): expm1 halvings and terms, sin/cos halvings and terms,
+    the atanh terms of log after its exponential reduction"""
+    import math
+
+    def ilog2(v):
+        return v.bit_length() - 1 if v > 1 else 0
+
+    need = 32 * NW + 8
+    s_e = math.isqrt(38 * NW)
+    T_e, bits = 1, 0
+    while bits < need:
+        T_e += 1
+        bits += s_e + ilog2(T_e)
+    s_c = max(4, (9 * math.isqrt(NW) - 5) // 2)
+    T_c, bits = 0, 0
+    while bits < need:
+        T_c += 1
+        bits += 2 * s_c + ilog2((2 * T_c) * (2 * T_c + 1))
+    T_l = (need + 2 * 48 - 1) // (2 * 48)  # atanh terms after the exp reduction
+    return s_e, T_e, s_c, T_c, T_l
+
+
 class DivSqrtWorkload(AxpyWorkload):
-    """z = x / y, sqrt(x) (correctly rounded: mpfr_div / mpfr_sqrt), exp(x) or
-    log(x) (faithful, the reference's contract) over n elements at precision
-    prec; the CPU baseline is the reference's own cu_fdiv / cu_sqrt / cu_exp /
-    cu_log built for the host."""
+    """z = x / y, sqrt(x) (correctly rounded: mpfr_div / mpfr_sqrt), exp(x),
+    log(x) or sin(x) (faithful, the reference's contract) over n elements at
+    precision prec; the CPU baseline is the reference's own cu_fdiv / cu_sqrt /
+    cu_exp / cu_log / cu_sin built for the host."""
 
     NAMES = {"div": ("correctly rounded divisions", "mp-div/s", "division z=x/y, RNDN (one rounding)"),
              "sqrt": ("correctly rounded square roots", "mp-sqrt/s", "square root z=sqrt(x), RNDN (one rounding)"),
              "exp": ("faithful exponentials", "mp-exp/s", "exponential z=exp(x), faithful (x in (-8, 8))"),
-             "log": ("faithful logarithms", "mp-log/s", "logarithm z=log(x), faithful (x > 0)")}
+             "log": ("faithful logarithms", "mp-log/s", "logarithm z=log(x), faithful (x > 0)"),
+             "sin": ("faithful sines", "mp-sin/s", "sine z=sin(x), faithful (x in (-32, 32))")}
 
     def __init__(self, name, op, prec, n, seed):
         super().__init__(name, False, prec, n, seed)
@@ -612,13 +637,13 @@ class DivSqrtWorkload(AxpyWorkload):
 
     @property
     def default_steps(self):  # about 1 s of GPU time: long enough for clock sampling
-        return {"div": 8000, "sqrt": 1300, "exp": 100, "log": 30}[self.op]
+        return {"div": 8000, "sqrt": 1300, "exp": 200, "log": 100, "sin": 100}[self.op]
 
     def make_host(self, rank):
         from mpc_cuda_b200 import layout, synth
 
         rng = np.random.default_rng(self.seed + 1000 * rank)
-        lo, hi = {"div": (-40, 40), "sqrt": (-40, 40), "exp": (-3, 3), "log": (-20, 20)}[self.op]
+        lo, hi = {"div": (-40, 40), "sqrt": (-40, 40), "exp": (-3, 3), "log": (-20, 20), "sin": (-5, 5)}[self.op]
         x = synth.random_elems(rng, self.prec, self.n, lo, hi)
         y = synth.random_elems(rng, self.prec, self.n, lo, hi)
         if self.op in ("sqrt", "log"):
@@ -631,6 +656,8 @@ class DivSqrtWorkload(AxpyWorkload):
         x, y, z = self.sets[i % self.nsets]
         if self.op == "div":
             self.M.div(self.prec, self.n, x, y, z, stream=stream)
+        elif self.op == "sin":
+            self.M.fmath("sin", self.prec, self.n, x, z, stream=stream)
         else:
             getattr(self.M, self.op)(self.prec, self.n, x, z, stream=stream)
 
@@ -652,25 +679,31 @@ class DivSqrtWorkload(AxpyWorkload):
         if self.op == "div":
             M.pack_aos(self.prec, self.n, self.dy_aos[s], self.ey, stream=stream)
             M.div(self.prec, self.n, self.ex, self.ey, self.ez, stream=stream)
+        elif self.op == "sin":
+            M.fmath("sin", self.prec, self.n, self.ex, self.ez, stream=stream)
         else:
             getattr(M, self.op)(self.prec, self.n, self.ex, self.ez, stream=stream)
         M.unpack_aos(self.prec, self.n, self.ez, self.dz_aos[s], stream=stream)
 
     def roofline(self, kernel_s, peaks, imad_ops_s):
         N = self.prec // 32
-        NW = N + 4  # exp / log working precision
+        NW = N + 4  # working precision of the elementary functions
+        s_e, T_e, s_c, T_c, T_l = _elem_params(NW)
         mulw, divw = rounded_product_imads(NW), 2 * NW * (NW + 2)
-        terms = 32 * NW // 17 + 3
-        exp_ops = terms * (mulw + divw) + 17 * mulw
-        # multiply-adds (lo + hi) per element: a long division is (N+2) quotient
-        # limbs x N; the square root runs about log2(32(N+1)/50) + 2 divisions of
-        # (2N+3) by (N+1) limbs; exp is the Taylor terms (a product and a division
-        # each) plus 16 squarings at N+4 limbs; log (away from 1) about
-        # log2(32(N+4)/20) Newton steps of one exp -- estimates: counts vary
+        dui = 5 * (NW + 2)  # division by a small integer: per quotient limb ~5
+        # multiply-adds (lo + hi) per element, from the implemented algorithms:
+        # a long division is (N+2) quotient limbs x N; the square root about
+        # log2(32(N+1)/50) + 2 divisions of (2N+3) by (N+1) limbs; at NW = N+4
+        # limbs exp is k ln2, T_e - 1 Taylor steps (a product and a small
+        # division), the last product and s_e doublings; log (away from 1) one
+        # exp, the product m exp(-y0), a division, T_l atanh steps and e ln2;
+        # sin two series of T_c steps and s_c doublings of two products --
+        # estimates: counts vary with the argument
         per = {"div": 2 * N * (N + 2),
                "sqrt": int(2 * (N + 1) * (N + 2) * (np.log2(32 * (N + 1) / 50.0) + 2)),
-               "exp": exp_ops,
-               "log": int((np.log2(32 * NW / 20.0) + 1) * (exp_ops + mulw))}[self.op]
+               "exp": (T_e - 1) * (mulw + dui) + (2 + s_e) * mulw,
+               "log": (T_e - 1) * (mulw + dui) + (1 + s_e) * mulw + divw + T_l * (mulw + dui) + 4 * mulw,
+               "sin": 2 * T_c * (mulw + dui) + 3 * mulw + 2 * s_c * mulw}[self.op]
         imad = per * self.n / kernel_s
         return {"bound": "imad", "achieved": round(imad / 1e9, 1),
                 "peak": round(imad_ops_s / 1e9, 1) if imad_ops_s else None, "unit": "Gop/s",
@@ -684,6 +717,8 @@ class DivSqrtWorkload(AxpyWorkload):
         kind = "ref" if impl == "ref" else "mp"
         if self.op == "div":
             O.div(self.prec, X[:count], Y[:count], impl=kind)
+        elif self.op == "sin":
+            O.fn("sin", self.prec, X[:count], impl=kind)
         else:
             getattr(O, self.op)(self.prec, X[:count], impl=kind)
         return count
@@ -691,7 +726,8 @@ class DivSqrtWorkload(AxpyWorkload):
     def config(self):
         return {"workload": self.desc, "prec": self.prec, "n": self.n,
                 "units": "one " + {"div": "correctly rounded division", "sqrt": "correctly rounded square root",
-                                   "exp": "faithful exponential", "log": "faithful logarithm"}[self.op],
+                                   "exp": "faithful exponential", "log": "faithful logarithm",
+                                   "sin": "faithful sine"}[self.op],
                 "l2": f"{self.nsets} rotating input sets > L2"}
 
 
@@ -700,6 +736,7 @@ WORKLOADS = {
     "sqrt_r512": lambda: DivSqrtWorkload("sqrt_r512", "sqrt", 512, 1 << 20, 0x5EED7),
     "exp_r512": lambda: DivSqrtWorkload("exp_r512", "exp", 512, 1 << 18, 0x5EED8),
     "log_r512": lambda: DivSqrtWorkload("log_r512", "log", 512, 1 << 18, 0x5EED9),
+    "sin_r512": lambda: DivSqrtWorkload("sin_r512", "sin", 512, 1 << 18, 0x5EEDA),
     "gemv_batch": lambda: GemvBatchWorkload("gemv_batch", 4096, 0x5EED4),
     "axpy_c1024": lambda: AxpyWorkload("axpy_c1024", True, 1024, 1 << 18, 0x5EED2),
     "axpy_r256": lambda: AxpyWorkload("axpy_r256", False, 256, 1 << 20, 0x5EED1),

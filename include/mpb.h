@@ -100,6 +100,57 @@ int mpb_sqrt_r(int prec, size_t n, const void *a, void *r, void *stream);
  * of |a| >= 2^29 (result outside the exponent range) and log of a <= 0 give 0. */
 int mpb_exp_r(int prec, size_t n, const void *a, void *r, void *stream);
 int mpb_log_r(int prec, size_t n, const void *a, void *r, void *stream);
+
+/* ---- elementary functions (reference include/mpc_cuda/cu_fmath.cuh:119-424,
+ * cu_fcmath.cuh:13-113; the drop-in cu_<name> of the C++ surface) ----
+ * Faithful (at most 1 ULP per component from the exact value; in practice
+ * correctly rounded), computed at 128 guard bits like the reference's.  Each
+ * function fn runs over n elements: r[i] = fn(a[i]) (pow and atan2 also read
+ * b[i]).  Values with no representation in the format (no NaN or infinity)
+ * give 0: exp / expm1 / sinh / cosh overflow (|a| >= 2^29), sin / cos / tan
+ * of |a| >= 2^30, log of a <= 0, log1p of a <= -1, atanh of |a| >= 1, pow of
+ * a negative a and a non-integer b, a complex division by zero.  asin of
+ * |a| >= 1 gives +-pi/2, acos of a >= 1 gives 0 and of a <= -1 pi (the
+ * reference's clamps, cu_fmath.cuh:382-399). */
+enum {
+  MPB_FN_EXP = 0,    /* cu_exp   cu_fmath.cuh:197 */
+  MPB_FN_LOG = 1,    /* cu_log   :214 */
+  MPB_FN_EXPM1 = 2,  /* cu_expm1 :234 */
+  MPB_FN_LOG1P = 3,  /* cu_log1p :247 */
+  MPB_FN_SIN = 4,    /* cu_sin   :293 */
+  MPB_FN_COS = 5,    /* cu_cos   :299 */
+  MPB_FN_TAN = 6,    /* cu_tan   :305 */
+  MPB_FN_ATAN = 7,   /* cu_atan  :329 */
+  MPB_FN_SINH = 8,   /* cu_sinh  :353 */
+  MPB_FN_COSH = 9,   /* cu_cosh  :356 */
+  MPB_FN_ATANH = 10, /* cu_atanh :373 */
+  MPB_FN_ASIN = 11,  /* cu_asin  :389 */
+  MPB_FN_ACOS = 12,  /* cu_acos  :401 */
+  MPB_FN_CBRT = 13,  /* cu_cbrt  :119 (sign kept) */
+  MPB_FN_POW = 14,   /* cu_pow(a, b) :420 */
+  MPB_FN_ATAN2 = 15  /* atan2(a, b) = the angle of (b, a), cu_fcmath.cuh:20 (cu_atan2_w) */
+};
+int mpb_fmath_r(int fn, int prec, size_t n, const void *a, const void *b, void *r, void *stream);
+/* complex (arrays of complex elements, each component faithful) */
+enum {
+  MPB_CFN_EXP = 0,  /* cu_cexp   cu_fcmath.cuh:47 */
+  MPB_CFN_LOG = 1,  /* cu_clog   :52 */
+  MPB_CFN_SQRT = 2, /* cu_csqrt  :58 (principal root) */
+  MPB_CFN_SIN = 3,  /* cu_csin   :74 */
+  MPB_CFN_COS = 4,  /* cu_ccos   :80 */
+  MPB_CFN_TAN = 5,  /* cu_ctan   :98 */
+  MPB_CFN_SINH = 6, /* cu_csinh  :86 */
+  MPB_CFN_COSH = 7, /* cu_ccosh  :92 */
+  MPB_CFN_DIV = 8   /* cu_cdiv(a, b) :42 */
+};
+int mpb_fmath_c(int fn, int prec, size_t n, const void *a, const void *b, void *r, void *stream);
+/* r[i] = round(a[i] / u), one rounding (mpfr_div_ui; the reference's
+ * cu_div_ui, cu_fmath.cuh:32-50, which is also correctly rounded); u = 0 gives 0 */
+int mpb_div_ui_r(int prec, size_t n, const void *a, uint64_t u, void *r, void *stream);
+/* r[0 .. n) = pi (which = MPB_CONST_PI) or ln 2 (MPB_CONST_LN2), correctly
+ * rounded (the reference's cu_pi / cu_ln2, cu_fmath.cuh:174-175) */
+enum { MPB_CONST_PI = 0, MPB_CONST_LN2 = 1 };
+int mpb_const_r(int which, int prec, size_t n, void *r, void *stream);
 /* complex r[i] = a[i]*b[i] + c[i], one rounding per component from exact
  * products (mpc_fma; the drop-in cu_cfma; no counterpart in the reference) */
 int mpb_fma_c(int prec, size_t n, const void *a, const void *b, const void *c, void *r, void *stream);

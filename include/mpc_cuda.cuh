@@ -1,7 +1,8 @@
 /* mpc_cuda.cuh -- drop-in umbrella for the fixed-precision path.
  *
  * Code written against the mpc_cuda umbrella (reference include/mpc_cuda.cuh:
- * 37-47) for its fixed-precision types keeps compiling unchanged:
+ * 37-55) for its fixed-precision types and their elementary functions keeps
+ * compiling unchanged:
  *
  *   #include "mpc_cuda.cuh"
  *   cu_fp::cu_freal<256> a = 1.5, b = x, c = a * b + a;
@@ -16,4 +17,5 @@
 #include "mpc_cuda/cu_freal.cuh"
 #include "mpc_cuda/cu_fcomplex.cuh"
 #include "mpc_cuda/cu_fmath.cuh"
+#include "mpc_cuda/cu_fcmath.cuh"
 #endif

@@ -62,6 +62,10 @@ _SIGS = {
     "mpb_sqrt_r": ([_I, _S, _V, _V, _V], C.c_int),
     "mpb_exp_r": ([_I, _S, _V, _V, _V], C.c_int),
     "mpb_log_r": ([_I, _S, _V, _V, _V], C.c_int),
+    "mpb_fmath_r": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
+    "mpb_fmath_c": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
+    "mpb_div_ui_r": ([_I, _S, _V, C.c_uint64, _V, _V], C.c_int),
+    "mpb_const_r": ([_I, _I, _S, _V, _V], C.c_int),
     "mpb_binop_c": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
     "mpb_axpy_r": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
     "mpb_axpy_c": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
@@ -129,6 +133,10 @@ def host_lib():
         H.mpbh_sqrt.argtypes = [_I, _L, _V, _V]
         H.mpbh_exp.argtypes = [_I, _L, _V, _V]
         H.mpbh_log.argtypes = [_I, _L, _V, _V]
+        for name in ("mpbh_fmath_r", "mpbh_fmath_c"):
+            getattr(H, name).argtypes = [_I, _I, _L, _V, _V, _V]
+        H.mpbh_div_ui.argtypes = [_I, _L, _V, C.c_ulonglong, _V]
+        H.mpbh_const.argtypes = [_I, _I, _V]
         for name in ("mpbh_axpy_r", "mpbh_axpy_c"):
             getattr(H, name).argtypes = [_I, _L, _V, _V, _V, _V]
         H.mpbh_from_double.argtypes = [_I, _L, _V, _V]
@@ -227,6 +235,34 @@ def exp(prec, n, a, r, stream=None):
 def log(prec, n, a, r, stream=None):
     """r = log(a), faithful (0 where a <= 0)."""
     _call("mpb_log_r", prec, n, _ptr(a), _ptr(r), _stream(stream))
+
+
+# elementary functions, in the order of mpb.h's MPB_FN_* / MPB_CFN_*
+FN = ("exp", "log", "expm1", "log1p", "sin", "cos", "tan", "atan", "sinh", "cosh",
+      "atanh", "asin", "acos", "cbrt", "pow", "atan2")
+CFN = ("exp", "log", "sqrt", "sin", "cos", "tan", "sinh", "cosh", "div")
+
+
+def fmath(name, prec, n, a, r, b=None, stream=None):
+    """r = name(a) (pow / atan2: name(a, b)), faithful; the drop-in cu_<name>."""
+    _call("mpb_fmath_r", FN.index(name), prec, n, _ptr(a), _ptr(b) if b is not None else None, _ptr(r),
+          _stream(stream))
+
+
+def cfmath(name, prec, n, a, r, b=None, stream=None):
+    """complex r = name(a) (div: a / b), each component faithful; cu_c<name>."""
+    _call("mpb_fmath_c", CFN.index(name), prec, n, _ptr(a), _ptr(b) if b is not None else None, _ptr(r),
+          _stream(stream))
+
+
+def div_ui(prec, n, a, u, r, stream=None):
+    """r = round(a / u) for an unsigned 64-bit integer u (cu_div_ui)."""
+    _call("mpb_div_ui_r", prec, n, _ptr(a), u, _ptr(r), _stream(stream))
+
+
+def const(which, prec, n, r, stream=None):
+    """r[0 .. n) = pi ('pi') or ln 2 ('ln2'), correctly rounded (cu_pi / cu_ln2)."""
+    _call("mpb_const_r", 0 if which == "pi" else 1, prec, n, _ptr(r), _stream(stream))
 
 
 def fma(prec, n, a, b, c, r, cplx=False, stream=None):

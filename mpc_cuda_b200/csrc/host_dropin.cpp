@@ -16,6 +16,12 @@
  *   mpbh_div(prec, n, a, b, r)           cu_fdiv
  *   mpbh_sqrt(prec, n, a, r)             cu_sqrt
  *   mpbh_exp / mpbh_log(prec, n, a, r)   cu_exp / cu_log
+ *   mpbh_fmath_r(fn, prec, n, a, b, r)   real elementary function fn (mpb.h
+ *                                        MPB_FN_*; b only for pow / atan2)
+ *   mpbh_fmath_c(fn, prec, n, a, b, r)   complex function fn (MPB_CFN_*;
+ *                                        b only for the division)
+ *   mpbh_div_ui(prec, n, a, u, r)        cu_div_ui
+ *   mpbh_const(which, prec, r)           cu_pi (0) / cu_ln2 (1)
  *   mpbh_axpy_r / mpbh_axpy_c(prec, n, a, x, y, z)
  *   mpbh_from_double / mpbh_to_double(prec, n, ...)
  * Return 0, or -1 for an unsupported precision.
@@ -81,6 +87,55 @@ void log1(long n, const void *A, void *R) {
   auto r = (cu_freal<PB> *)R;
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < n; i++) r[i] = cu_fp::cu_log<PB>(a[i]);
+}
+template <int PB>
+cu_freal<PB> fmath1(int fn, const cu_freal<PB> &a, const cu_freal<PB> &b) {
+  using namespace cu_fp;
+  switch (fn) {
+    case 0: return cu_exp<PB>(a);
+    case 1: return cu_log<PB>(a);
+    case 2: return cu_expm1<PB>(a);
+    case 3: return cu_log1p<PB>(a);
+    case 4: return cu_sin<PB>(a);
+    case 5: return cu_cos<PB>(a);
+    case 6: return cu_tan<PB>(a);
+    case 7: return cu_atan<PB>(a);
+    case 8: return cu_sinh<PB>(a);
+    case 9: return cu_cosh<PB>(a);
+    case 10: return cu_atanh<PB>(a);
+    case 11: return cu_asin<PB>(a);
+    case 12: return cu_acos<PB>(a);
+    case 13: return cu_cbrt<PB>(a);
+    case 14: return cu_pow<PB>(a, b);
+    default: return cu_atan2<PB>(a, b);
+  }
+}
+template <int PB>
+void fmath_r(int fn, long n, const void *A, const void *B, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto b = (const cu_freal<PB> *)B;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (long i = 0; i < n; i++) r[i] = fmath1<PB>(fn, a[i], b ? b[i] : a[i]);
+}
+template <int PB>
+void fmath_c(int fn, long n, const void *A, const void *B, void *R) {
+  auto a = (const cu_fcomplex<PB> *)A;
+  auto b = (const cu_fcomplex<PB> *)B;
+  auto r = (cu_fcomplex<PB> *)R;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (long i = 0; i < n; i++) r[i] = fn == 8 ? cu_fp::cu_cdiv<PB>(a[i], b[i]) : cu_fp::detail::cfunc<PB>(fn, a[i]);
+}
+template <int PB>
+void div_ui1(long n, const void *A, unsigned long long u, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_div_ui<PB>(a[i], u);
+}
+template <int PB>
+void const1(int which, void *R) {
+  *(cu_freal<PB> *)R = which == 0 ? cu_fp::cu_pi<PB>() : cu_fp::cu_ln2<PB>();
 }
 template <int PB>
 void cfma3(long n, const void *A, const void *B, const void *C, void *R) {
@@ -171,6 +226,18 @@ int mpbh_sqrt(int prec, long n, const void *a, void *r) {
 }
 int mpbh_exp(int prec, long n, const void *a, void *r) { MPBH_DISPATCH(prec, exp1<PB>(n, a, r)) }
 int mpbh_log(int prec, long n, const void *a, void *r) { MPBH_DISPATCH(prec, log1<PB>(n, a, r)) }
+int mpbh_fmath_r(int fn, int prec, long n, const void *a, const void *b, void *r) {
+  if (fn < 0 || fn > 15 || ((fn == 14 || fn == 15) && !b)) return -2;
+  MPBH_DISPATCH(prec, fmath_r<PB>(fn, n, a, b, r))
+}
+int mpbh_fmath_c(int fn, int prec, long n, const void *a, const void *b, void *r) {
+  if (fn < 0 || fn > 8 || (fn == 8 && !b)) return -2;
+  MPBH_DISPATCH(prec, fmath_c<PB>(fn, n, a, b, r))
+}
+int mpbh_div_ui(int prec, long n, const void *a, unsigned long long u, void *r) {
+  MPBH_DISPATCH(prec, div_ui1<PB>(n, a, u, r))
+}
+int mpbh_const(int which, int prec, void *r) { MPBH_DISPATCH(prec, const1<PB>(which, r)) }
 int mpbh_cfma(int prec, long n, const void *a, const void *b, const void *c, void *r) {
   MPBH_DISPATCH(prec, cfma3<PB>(n, a, b, c, r))
 }

@@ -58,6 +58,10 @@ def lib():
         L.mp_sqrt.argtypes = [it, lg, vp, vp]
         L.mp_exp.argtypes = [it, it, lg, vp, vp]
         L.mp_log.argtypes = [it, it, lg, vp, vp]
+        for name in ("mp_fn", "mp_cfn"):
+            getattr(L, name).argtypes = [it, it, it, lg, vp, vp, vp]
+        L.mp_div_ui.argtypes = [it, lg, vp, C.c_ulong, vp]
+        L.mp_const.argtypes = [it, it, vp]
         for name in ("orc_fma", "mp_fma", "mp_cfma", "mp_cfma_dot"):
             getattr(L, name).argtypes = [it, lg, vp, vp, vp, vp]
         for name in ("orc_axpy_r", "orc_axpy_c", "mp_axpy_r", "mp_axpy_c"):
@@ -111,6 +115,8 @@ def ref():
         R.ref_sqrt.argtypes = [it, lg, vp, vp]
         R.ref_exp.argtypes = [it, lg, vp, vp]
         R.ref_log.argtypes = [it, lg, vp, vp]
+        for name in ("ref_fn", "ref_cfn"):
+            getattr(R, name).argtypes = [it, it, lg, vp, vp, vp]
         R.ref_from_double.argtypes = [it, lg, vp, vp]
         R.ref_to_double.argtypes = [it, lg, vp, vp]
         R.ref_elem_bytes.argtypes = [it]
@@ -135,6 +141,30 @@ def gen_pairs(prec: int, n: int, seed: int, cplx: bool = False):
     f = lib().orc_gen_pairs_c if cplx else lib().orc_gen_pairs_r
     f(prec, n, seed, _p(A), _p(B))
     return A, B
+
+
+def rand_elems(prec: int, n: int, seed: int, elo: int, ehi: int, positive: bool = False,
+               cplx: bool = False) -> np.ndarray:
+    """n random elements in the reference's test layout (tools/test_fmath.cu:
+    14-20 randf): full-width random significands (top bit set, the bits below
+    PB clear), exponents uniform in [elo, ehi], random signs unless positive."""
+    rng = np.random.default_rng(seed)
+    n64, es = (prec + 63) // 64, elem_bytes(prec)
+    parts = []
+    for _ in range(2 if cplx else 1):
+        m = rng.integers(0, 1 << 63, size=(n, n64), dtype=np.uint64) * np.uint64(2) + \
+            rng.integers(0, 2, size=(n, n64), dtype=np.uint64)
+        m[:, -1] |= np.uint64(1 << 63)
+        sb = 64 * n64 - prec
+        if sb:
+            m[:, 0] &= ~np.uint64((1 << sb) - 1)
+        E = np.zeros((n, es), np.uint8)
+        sign = np.ones(n, np.int32) if positive else rng.choice(np.array([-1, 1], np.int32), n)
+        E[:, 0:4] = sign.view(np.uint8).reshape(n, 4)
+        E[:, 8:16] = rng.integers(elo, ehi + 1, n).astype(np.int64).view(np.uint8).reshape(n, 8)
+        E[:, 16:] = m.view(np.uint8).reshape(n, 8 * n64)
+        parts.append(E)
+    return np.concatenate(parts, axis=1) if cplx else parts[0]
 
 
 def mismatches(prec: int, X: np.ndarray, Y: np.ndarray, cplx: bool = False):
@@ -204,6 +234,57 @@ def log(prec: int, A, out_prec: int | None = None, impl: str = "mp") -> np.ndarr
         ref().ref_log(prec, A.shape[0], _p(A), _p(R))
     else:
         lib().mp_log(prec, po, A.shape[0], _p(A), _p(R))
+    return R
+
+
+# elementary functions, numbered as the engine's MPB_FN_* / MPB_CFN_*
+FN = ("exp", "log", "expm1", "log1p", "sin", "cos", "tan", "atan", "sinh", "cosh",
+      "atanh", "asin", "acos", "cbrt", "pow", "atan2")
+CFN = ("exp", "log", "sqrt", "sin", "cos", "tan", "sinh", "cosh", "div")
+
+
+def fn(name: str, prec: int, A, B=None, out_prec: int | None = None, impl: str = "mp") -> np.ndarray:
+    """Real function ``name`` (FN; pow / atan2 take B): 'mp' = MPFR rounded at
+    out_prec bits (default prec); 'ref' = the reference's own cu_fmath
+    function built for the host (at prec)."""
+    f = FN.index(name)
+    n = A.shape[0]
+    po = prec if impl == "ref" else (out_prec or prec)
+    R = empty(po, n)
+    pb = _p(B) if B is not None else None
+    if impl == "ref":
+        ref().ref_fn(f, prec, n, _p(A), pb, _p(R))
+    else:
+        lib().mp_fn(f, prec, po, n, _p(A), pb, _p(R))
+    return R
+
+
+def cfn(name: str, prec: int, A, B=None, out_prec: int | None = None, impl: str = "mp") -> np.ndarray:
+    """Complex function ``name`` (CFN; div takes B): 'mp' = MPC (each component
+    rounded to nearest at out_prec bits); 'ref' = the reference's cu_fcmath."""
+    f = CFN.index(name)
+    n = A.shape[0]
+    po = prec if impl == "ref" else (out_prec or prec)
+    R = empty(po, n, True)
+    pb = _p(B) if B is not None else None
+    if impl == "ref":
+        ref().ref_cfn(f, prec, n, _p(A), pb, _p(R))
+    else:
+        lib().mp_cfn(f, prec, po, n, _p(A), pb, _p(R))
+    return R
+
+
+def div_ui(prec: int, A, u: int) -> np.ndarray:
+    """round(a / u), mpfr_div_ui (RNDN)."""
+    R = empty(prec, A.shape[0])
+    lib().mp_div_ui(prec, A.shape[0], _p(A), u, _p(R))
+    return R
+
+
+def const(which: str, prec: int) -> np.ndarray:
+    """pi or ln2 rounded to nearest at prec bits (mpfr_const_pi / _log2)."""
+    R = empty(prec, 1)
+    lib().mp_const(0 if which == "pi" else 1, prec, _p(R))
     return R
 
 

@@ -990,6 +990,59 @@ static void mp_un(mpfr_un_t f, int P, int Pout, long n, const void *A, void *R) 
 void mp_exp(int P, int Pout, long n, const void *A, void *R) { mp_un(mpfr_exp, P, Pout, n, A, R); }
 void mp_log(int P, int Pout, long n, const void *A, void *R) { mp_un(mpfr_log, P, Pout, n, A, R); }
 
+/* the real elementary functions at precision Pout, fn numbered as the
+ * engine's MPB_FN_* (0 exp .. 13 cbrt unary; 14 pow(a, b), 15 atan2(a, b)):
+ * the checker for the faithful drop-in cu_exp .. cu_pow of the reference's
+ * cu_fmath.cuh (its tools/test_fmath.cu and test_fmath3.cu compare the same
+ * functions with MPFR) */
+typedef int (*mpfr_bin_t)(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *, shim_rnd_t);
+int mp_fn(int fn, int P, int Pout, long n, const void *A, const void *B, void *R) {
+  static const mpfr_un_t un[14] = {mpfr_exp,  mpfr_log,  mpfr_expm1, mpfr_log1p, mpfr_sin,  mpfr_cos,  mpfr_tan,
+                                   mpfr_atan, mpfr_sinh, mpfr_cosh,  mpfr_atanh, mpfr_asin, mpfr_acos, mpfr_cbrt};
+  if (fn < 0 || fn > 15) return -1;
+  if (fn < 14) {
+    mp_un(un[fn], P, Pout, n, A, R);
+    return 0;
+  }
+  const mpfr_bin_t f = fn == 14 ? mpfr_pow : mpfr_atan2;
+  size_t es = esz_of(P), eo = esz_of(Pout);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    shim_mpfr_t a, b, r;
+    as_mpfr(P, a, cat(A, es, i));
+    as_mpfr(P, b, cat(B, es, i));
+    mpfr_init2(r, Pout);
+    f(r, a, b, SHIM_RNDN);
+    store_mpfr(Pout, at(R, eo, i), r);
+    mpfr_clear(r);
+  }
+  return 0;
+}
+
+/* round(a / u) (mpfr_div_ui), and pi / ln 2 (which 0 / 1) at precision P */
+void mp_div_ui(int P, long n, const void *A, unsigned long u, void *R) {
+  size_t es = esz_of(P);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    shim_mpfr_t a, r;
+    as_mpfr(P, a, cat(A, es, i));
+    mpfr_init2(r, P);
+    mpfr_div_ui(r, a, u, SHIM_RNDN);
+    store_mpfr(P, at(R, es, i), r);
+    mpfr_clear(r);
+  }
+}
+void mp_const(int which, int P, void *R) {
+  shim_mpfr_t r;
+  mpfr_init2(r, P);
+  if (which == 0)
+    mpfr_const_pi(r, SHIM_RNDN);
+  else
+    mpfr_const_log2(r, SHIM_RNDN);
+  store_mpfr(P, (elem_t *)R, r);
+  mpfr_clear(r);
+}
+
 void mp_sqrt(int P, long n, const void *A, void *R) {
   size_t es = esz_of(P);
 #pragma omp parallel for schedule(static)
@@ -1049,6 +1102,34 @@ void mp_csub(int P, long n, const void *A, const void *B, void *R) { mp_cbin(mpc
 /* complex fused multiply-add a*b + c, one rounding per component: the
  * system mpc_fma, and independently mpc_dot over ([a, c], [b, 1]); the
  * reference has no such operation (checker for the engine's cu_cfma) */
+/* the complex elementary functions at precision Pout (each component
+ * rounded to nearest, MPC_RNDNN), fn numbered as the engine's MPB_CFN_*
+ * (0 exp, 1 log, 2 sqrt, 3 sin, 4 cos, 5 tan, 6 sinh, 7 cosh, 8 a / b): the
+ * checker for the drop-in cu_cexp .. cu_cdiv of the reference's
+ * cu_fcmath.cuh (its tools/test_fcmath.cu compares them with MPC) */
+typedef int (*mpc_un_t)(shim_mpc_ptr, const shim_mpc_struct *, int);
+int mp_cfn(int fn, int P, int Pout, long n, const void *A, const void *B, void *R) {
+  static const mpc_un_t un[8] = {mpc_exp, mpc_log, mpc_sqrt, mpc_sin, mpc_cos, mpc_tan, mpc_sinh, mpc_cosh};
+  if (fn < 0 || fn > 8) return -1;
+  size_t es = 2 * esz_of(P), eo = 2 * esz_of(Pout);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    shim_mpc_t a, b, r;
+    as_mpc(P, a, cat(A, es, i));
+    mpc_init2(r, Pout);
+    if (fn == 8) {
+      as_mpc(P, b, cat(B, es, i));
+      mpc_div(r, a, b, SHIM_MPC_RNDNN);
+    } else {
+      un[fn](r, a, SHIM_MPC_RNDNN);
+    }
+    store_mpfr(Pout, RE(at(R, eo, i)), r->re);
+    store_mpfr(Pout, IM(at(R, eo, i), esz_of(Pout)), r->im);
+    mpc_clear(r);
+  }
+  return 0;
+}
+
 void mp_cfma(int P, long n, const void *A, const void *B, const void *C, void *R) {
   size_t es = 2 * esz_of(P);
 #pragma omp parallel for schedule(static)

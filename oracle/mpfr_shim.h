@@ -69,6 +69,23 @@ int mpfr_div(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *, 
 int mpfr_sqrt(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
 int mpfr_exp(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
 int mpfr_log(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_expm1(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_log1p(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_sin(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_cos(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_tan(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_atan(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_sinh(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_cosh(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_atanh(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_asin(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_acos(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_cbrt(shim_mpfr_ptr, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_pow(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_atan2(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *, shim_rnd_t);
+int mpfr_div_ui(shim_mpfr_ptr, const shim_mpfr_struct *, unsigned long, shim_rnd_t);
+int mpfr_const_pi(shim_mpfr_ptr, shim_rnd_t);
+int mpfr_const_log2(shim_mpfr_ptr, shim_rnd_t);
 int mpfr_fma(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *,
              const shim_mpfr_struct *, shim_rnd_t);
 int mpfr_fmms(shim_mpfr_ptr, const shim_mpfr_struct *, const shim_mpfr_struct *,
@@ -90,6 +107,15 @@ int mpc_fma(shim_mpc_ptr, const shim_mpc_struct *, const shim_mpc_struct *,
             const shim_mpc_struct *, int);
 int mpc_dot(shim_mpc_ptr, const shim_mpc_ptr *, const shim_mpc_ptr *, unsigned long, int);
 int mpc_cmp(const shim_mpc_struct *, const shim_mpc_struct *);
+int mpc_div(shim_mpc_ptr, const shim_mpc_struct *, const shim_mpc_struct *, int);
+int mpc_exp(shim_mpc_ptr, const shim_mpc_struct *, int);
+int mpc_log(shim_mpc_ptr, const shim_mpc_struct *, int);
+int mpc_sqrt(shim_mpc_ptr, const shim_mpc_struct *, int);
+int mpc_sin(shim_mpc_ptr, const shim_mpc_struct *, int);
+int mpc_cos(shim_mpc_ptr, const shim_mpc_struct *, int);
+int mpc_tan(shim_mpc_ptr, const shim_mpc_struct *, int);
+int mpc_sinh(shim_mpc_ptr, const shim_mpc_struct *, int);
+int mpc_cosh(shim_mpc_ptr, const shim_mpc_struct *, int);
 
 #ifdef __cplusplus
 }

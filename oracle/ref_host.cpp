@@ -18,6 +18,7 @@
 #include <cstring>
 #include "mpc_cuda/cu_fcomplex.cuh"
 #include "mpc_cuda/cu_fmath.cuh"
+#include "mpc_cuda/cu_fcmath.cuh"
 
 using cu_fp::cu_fcomplex;
 using cu_fp::cu_freal;
@@ -209,6 +210,63 @@ void t_to_double(long n, const void *X, double *d) {
 
 /* runtime precision -> template instantiation (the reference's test set,
  * tools/test_freal.cu:92-102, plus the engine's PB list) */
+/* the reference's elementary functions, numbered as the engine's MPB_FN_* /
+ * MPB_CFN_* (its cu_atan2 exists only at working precision, cu_atan2_w) */
+template <int PB>
+void t_fn(int fn, long n, const void *A, const void *B, void *R) {
+  using namespace cu_fp;
+  auto a = (const cu_freal<PB> *)A;
+  auto b = (const cu_freal<PB> *)B;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (long i = 0; i < n; i++) {
+    const cu_freal<PB> x = a[i];
+    switch (fn) {
+      case 0: r[i] = cu_exp<PB>(x); break;
+      case 1: r[i] = cu_log<PB>(x); break;
+      case 2: r[i] = cu_expm1<PB>(x); break;
+      case 3: r[i] = cu_log1p<PB>(x); break;
+      case 4: r[i] = cu_sin<PB>(x); break;
+      case 5: r[i] = cu_cos<PB>(x); break;
+      case 6: r[i] = cu_tan<PB>(x); break;
+      case 7: r[i] = cu_atan<PB>(x); break;
+      case 8: r[i] = cu_sinh<PB>(x); break;
+      case 9: r[i] = cu_cosh<PB>(x); break;
+      case 10: r[i] = cu_atanh<PB>(x); break;
+      case 11: r[i] = cu_asin<PB>(x); break;
+      case 12: r[i] = cu_acos<PB>(x); break;
+      case 13: r[i] = cu_cbrt<PB>(x); break;
+      case 14: r[i] = cu_pow<PB>(x, b[i]); break;
+      default: {
+        const int W = PB + CU_FGUARD;
+        r[i] = cu_convert<PB>(cu_atan2_w<W>(cu_convert<W>(x), cu_convert<W>(b[i])));
+      }
+    }
+  }
+}
+template <int PB>
+void t_cfn(int fn, long n, const void *A, const void *B, void *R) {
+  using namespace cu_fp;
+  auto a = (const cu_fcomplex<PB> *)A;
+  auto b = (const cu_fcomplex<PB> *)B;
+  auto r = (cu_fcomplex<PB> *)R;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (long i = 0; i < n; i++) {
+    const cu_fcomplex<PB> z = a[i];
+    switch (fn) {
+      case 0: r[i] = cu_cexp<PB>(z); break;
+      case 1: r[i] = cu_clog<PB>(z); break;
+      case 2: r[i] = cu_csqrt<PB>(z); break;
+      case 3: r[i] = cu_csin<PB>(z); break;
+      case 4: r[i] = cu_ccos<PB>(z); break;
+      case 5: r[i] = cu_ctan<PB>(z); break;
+      case 6: r[i] = cu_csinh<PB>(z); break;
+      case 7: r[i] = cu_ccosh<PB>(z); break;
+      default: r[i] = cu_cdiv<PB>(z, b[i]);
+    }
+  }
+}
+
 #define REF_DISPATCH(P, CALL)                                                                   \
   switch (P) {                                                                                  \
     case 32: { constexpr int PB = 32; CALL; } return 0;                                         \
@@ -235,6 +293,12 @@ int ref_div(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH
 int ref_sqrt(int P, long n, const void *A, void *R) { REF_DISPATCH(P, t_sqrt<PB>(n, A, R)) }
 int ref_exp(int P, long n, const void *A, void *R) { REF_DISPATCH(P, t_exp<PB>(n, A, R)) }
 int ref_log(int P, long n, const void *A, void *R) { REF_DISPATCH(P, t_log<PB>(n, A, R)) }
+int ref_fn(int fn, int P, long n, const void *A, const void *B, void *R) {
+  REF_DISPATCH(P, t_fn<PB>(fn, n, A, B, R))
+}
+int ref_cfn(int fn, int P, long n, const void *A, const void *B, void *R) {
+  REF_DISPATCH(P, t_cfn<PB>(fn, n, A, B, R))
+}
 int ref_sub(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_sub<PB>(n, A, B, R)) }
 int ref_cmul(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_cmul<PB>(n, A, B, R)) }
 int ref_cadd(int P, long n, const void *A, const void *B, void *R) { REF_DISPATCH(P, t_cadd<PB>(n, A, B, R)) }

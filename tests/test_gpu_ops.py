@@ -293,3 +293,92 @@ def test_gemm_real_pb512_rows_sample(orc, mpb):
     last = orc.gemm(prec, m, n, k, A, k, B, n, rows=(m - 2, m))
     assert orc.mismatches(prec, got[(m - 2) * n:], last[(m - 2) * n:])[0] == 0
     assert es == layout.aos_bytes(prec)
+
+
+# ---------------------------------------------------------------- elementary functions
+def _fmath_args(orc, prec, seed):
+    """per function: random arguments in the reference's ranges plus the hard set"""
+    import fmath_cases as fc
+
+    M = 600 if prec <= 512 else 160
+    hard = fc.hard_args(orc, prec, seed)
+    out = {}
+    for i, name in enumerate(fc.FN):
+        A, B = fc.random_args(orc, name, prec, M, seed + 7 * i)
+        if name in hard:
+            A = np.concatenate([A, hard[name]])
+        elif B is not None:
+            A2, B2 = fc.random_args(orc, name, prec, 64, seed + 7 * i + 3)
+            A, B = np.concatenate([A, A2]), np.concatenate([B, B2])
+        out[name] = (A, B)
+    return out
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_fmath_real(orc, mpb, prec):
+    """mpb_fmath_r, every function: bit-identical to the host build of the
+    same drop-in functions (which tests/test_host_dropin.py holds to MPFR),
+    and within 1 ULP of MPFR at 4 PB."""
+    import ctypes as C
+
+    import fmath_cases as fc
+
+    H = mpb.host_lib()
+    pref = min(4 * prec, orc.lib().orc_max_prec())
+    for name, (A, B) in _fmath_args(orc, prec, 0x7100 + prec).items():
+        M = A.shape[0]
+        r = mpb.empty(prec, M)
+        mpb.fmath(name, prec, M, dvec(prec, A), r, b=dvec(prec, B) if B is not None else None)
+        got = hvec(prec, r, M)
+        host = orc.empty(prec, M)
+        H.mpbh_fmath_r(fc.FN.index(name), prec, M, A.ctypes.data_as(C.c_void_p),
+                       B.ctypes.data_as(C.c_void_p) if B is not None else None, host.ctypes.data_as(C.c_void_p))
+        bad, first = orc.mismatches(prec, got, host)
+        assert bad == 0, f"{name} PB={prec}: device differs from host build at {first}"
+        ulp = orc.ulp_errors(prec, got, pref, orc.fn(name, prec, A, B, pref))
+        assert ulp.max() <= 1.0, f"{name} PB={prec}: {ulp.max():.3g} ULP"
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_fmath_complex(orc, mpb, prec):
+    """mpb_fmath_c, every function: bit-identical to the host build, each
+    component within 1 ULP of MPC at 4 PB."""
+    import ctypes as C
+
+    import fmath_cases as fc
+
+    H = mpb.host_lib()
+    M = 300 if prec <= 512 else 80
+    es, pref = orc.elem_bytes(prec), min(4 * prec, orc.lib().orc_max_prec())
+    eo = orc.elem_bytes(pref)
+    for i, name in enumerate(fc.CFN):
+        A = orc.rand_elems(prec, M, 0x7300 + 16 * prec + i, -3, 3, cplx=True)
+        B = orc.rand_elems(prec, M, 0x7400 + 16 * prec + i, -3, 3, cplx=True) if name == "div" else None
+        r = mpb.empty(prec, M, True)
+        mpb.cfmath(name, prec, M, dvec(prec, A, True), r, b=dvec(prec, B, True) if B is not None else None)
+        got = hvec(prec, r, M, True)
+        host = orc.empty(prec, M, True)
+        H.mpbh_fmath_c(i, prec, M, A.ctypes.data_as(C.c_void_p), B.ctypes.data_as(C.c_void_p) if B is not None else None,
+                       host.ctypes.data_as(C.c_void_p))
+        assert orc.mismatches(prec, got, host, True)[0] == 0, f"c{name} PB={prec}: device differs from host build"
+        ref = orc.cfn(name, prec, A, B, pref)
+        for c in (0, 1):
+            ulp = orc.ulp_errors(prec, got[:, c * es:(c + 1) * es], pref, ref[:, c * eo:(c + 1) * eo])
+            assert ulp.max() <= 1.0, f"c{name} PB={prec} component {c}: {ulp.max():.3g} ULP"
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_div_ui_and_constants(orc, mpb, prec):
+    """mpb_div_ui_r and mpb_const_r bit-identical to mpfr_div_ui and
+    mpfr_const_pi / mpfr_const_log2."""
+    A, _ = orc.gen_pairs(prec, 3000, 0xD7 + prec)
+    a = dvec(prec, A)
+    for u in (3, 10, 2 ** 32 - 1, 2 ** 40 + 3, 2 ** 64 - 1):
+        r = mpb.empty(prec, A.shape[0])
+        mpb.div_ui(prec, A.shape[0], a, u, r)
+        assert orc.mismatches(prec, hvec(prec, r, A.shape[0]), orc.div_ui(prec, A, u))[0] == 0, f"u={u}"
+    for which in ("pi", "ln2"):
+        r = mpb.empty(prec, 40)
+        mpb.const(which, prec, 40, r)
+        want = np.repeat(orc.const(which, prec), 40, axis=0)
+        assert orc.mismatches(prec, hvec(prec, r, 40), want)[0] == 0, which

@@ -298,3 +298,104 @@ def test_sample_fixed_known_values(mpb):
     out = np.zeros(2)
     H.mpbh_to_double(prec, 2, _p(r.reshape(2, es).copy()), _p(out))
     assert tuple(out) == (3.625, -0.5)
+
+
+# ---------------------------------------------------------------- elementary functions
+def _fmath_host(H, orc, name, prec, A, B=None):
+    import fmath_cases as fc
+
+    R = orc.empty(prec, A.shape[0])
+    rc = H.mpbh_fmath_r(fc.FN.index(name), prec, A.shape[0], _p(A), _p(B) if B is not None else None, _p(R))
+    assert rc == 0
+    return R
+
+
+def _check_faithful(orc, prec, name, R, A, B=None, label="", cr=True):
+    """at most 1 ULP from MPFR at 4 PB (the reference's contract); on random
+    arguments (cr) also equal to MPFR's correctly rounded value on nearly
+    every one -- structured arguments (the hard sets) can sit arbitrarily
+    close to a rounding boundary, where a faithful result may differ"""
+    pref = min(4 * prec, orc.lib().orc_max_prec())
+    ulp = orc.ulp_errors(prec, R, pref, orc.fn(name, prec, A, B, pref))
+    assert ulp.max() <= 1.0, f"{name}{label} PB={prec}: {ulp.max():.3g} ULP at {int(ulp.argmax())}"
+    if cr:
+        bad = orc.mismatches(prec, R, orc.fn(name, prec, A, B))[0]
+        assert bad <= A.shape[0] // 100, f"{name}{label} PB={prec}: {bad} not correctly rounded"
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_fmath_real_faithful(orc, mpb, prec):
+    """cu_exp .. cu_pow (and atan2) on the reference's test ranges
+    (tools/test_fmath.cu, test_fmath3.cu) and on the hard argument sets."""
+    import fmath_cases as fc
+
+    H = mpb.host_lib()
+    M = 120 if prec <= 1056 else 40
+    hard = fc.hard_args(orc, prec, 0xF0 + prec)
+    for i, name in enumerate(fc.FN):
+        A, B = fc.random_args(orc, name, prec, M, 0x3000 + 16 * prec + i)
+        _check_faithful(orc, prec, name, _fmath_host(H, orc, name, prec, A, B), A, B)
+        if name in hard:
+            Hd = hard[name]
+            _check_faithful(orc, prec, name, _fmath_host(H, orc, name, prec, Hd), Hd, label=" (hard set)", cr=False)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_fmath_complex_faithful(orc, mpb, prec):
+    """cu_cexp .. cu_cdiv: each component within 1 ULP of MPC at 4 PB."""
+    import fmath_cases as fc
+
+    H = mpb.host_lib()
+    M = 80 if prec <= 1056 else 24
+    es, pref = orc.elem_bytes(prec), min(4 * prec, orc.lib().orc_max_prec())
+    eo = orc.elem_bytes(pref)
+    for i, name in enumerate(fc.CFN):
+        A = orc.rand_elems(prec, M, 0x5000 + 16 * prec + i, -3, 3, cplx=True)
+        B = orc.rand_elems(prec, M, 0x6000 + 16 * prec + i, -3, 3, cplx=True) if name == "div" else None
+        R = orc.empty(prec, M, True)
+        assert H.mpbh_fmath_c(i, prec, M, _p(A), _p(B) if B is not None else None, _p(R)) == 0
+        ref = orc.cfn(name, prec, A, B, pref)
+        for c in (0, 1):
+            ulp = orc.ulp_errors(prec, R[:, c * es:(c + 1) * es], pref, ref[:, c * eo:(c + 1) * eo])
+            assert ulp.max() <= 1.0, f"c{name} PB={prec} component {c}: {ulp.max():.3g} ULP"
+        assert orc.mismatches(prec, R, orc.cfn(name, prec, A, B), True)[0] <= M // 50, f"c{name} PB={prec}"
+
+
+@pytest.mark.parametrize("prec", (64, 256, 1056))
+def test_fmath_special_values(orc, mpb, prec):
+    """The documented edges: no value in the format gives 0; the reference's
+    asin / acos clamps; exact cases (pow with an integer exponent, cbrt)."""
+    import fmath_cases as fc
+
+    H = mpb.host_lib()
+    pi = orc.const("pi", prec)
+
+    def scaled_pi(sign, shift):
+        e = pi.copy()
+        e[0, 0:4] = np.array([sign], np.int32).view(np.uint8)
+        e[0, 8:16] = np.array([pi[0, 8:16].view(np.int64)[0] + shift], np.int64).view(np.uint8)
+        return e
+
+    named = {"pi": scaled_pi(1, 0), "pi/2": scaled_pi(1, -1), "-pi/2": scaled_pi(-1, -1), "pi/4": scaled_pi(1, -2)}
+    for name, args, want in fc.special_args():
+        A = orc.from_double(prec, [args[0]])
+        B = orc.from_double(prec, [args[1]]) if len(args) > 1 else None
+        got = _fmath_host(H, orc, name, prec, A, B)
+        exp = named[want] if isinstance(want, str) else orc.from_double(prec, [want])
+        assert orc.mismatches(prec, got, exp)[0] == 0, f"{name}{args} PB={prec}"
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_div_ui_and_constants(orc, mpb, prec):
+    """cu_div_ui (32- and 64-bit divisors) bit-identical to mpfr_div_ui, and
+    cu_pi / cu_ln2 to mpfr_const_pi / mpfr_const_log2."""
+    H = mpb.host_lib()
+    A, _ = orc.gen_pairs(prec, 400, 0xD1 + prec)
+    for u in (1, 3, 7, 10, 2 ** 31 + 11, 2 ** 32 - 1, 2 ** 32 + 15, 12345678901234567, 2 ** 64 - 1):
+        R = orc.empty(prec, A.shape[0])
+        assert H.mpbh_div_ui(prec, A.shape[0], _p(A), u, _p(R)) == 0
+        assert orc.mismatches(prec, R, orc.div_ui(prec, A, u))[0] == 0, f"u={u}"
+    for k, which in enumerate(("pi", "ln2")):
+        R = orc.empty(prec, 1)
+        assert H.mpbh_const(k, prec, _p(R)) == 0
+        assert orc.mismatches(prec, R, orc.const(which, prec))[0] == 0, which
