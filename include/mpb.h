@@ -77,6 +77,20 @@ int mpb_unpack_aos(int prec, size_t n, const void *vec, void *aos, void *stream)
 /* AoS cu_fcomplex<prec>[n] <-> complex tiled vector (reference cu_fcomplex.cuh:98-113) */
 int mpb_cpack_aos(int prec, size_t n, const void *aos, void *cvec, void *stream);
 int mpb_cunpack_aos(int prec, size_t n, const void *cvec, void *aos, void *stream);
+/* ---- host interop with MPFR / MPC objects (host memory, no GPU, no MPFR link) ----
+ * dst[i] / src[i] point to initialised mpfr_t (mpfr_ptr) or mpc_t objects; AoS
+ * arrays are cu_freal<prec> / cu_fcomplex<prec> in host memory.  To MPFR: the
+ * value rounded to nearest-even at the destination's own precision (exact
+ * when it is >= prec), the reference's to_mpfr (tools/test_freal.cu:28-39:
+ * mpz_import, mpfr_set_z RNDN, mpfr_mul_2si).  From MPFR: rounded to
+ * nearest-even at prec bits; -0 becomes +0; NaN, infinities and exponents
+ * outside +-2^30 return MPB_ERR_ARG.  No counterpart in the reference's
+ * library (its tests carry their own converters). */
+int mpb_aos_to_mpfr(int prec, size_t n, const void *aos, void *const *dst);
+int mpb_aos_from_mpfr(int prec, size_t n, const void *const *src, void *aos);
+int mpb_caos_to_mpc(int prec, size_t n, const void *caos, void *const *dst);
+int mpb_caos_from_mpc(int prec, size_t n, const void *const *src, void *caos);
+
 /* double[n] -> vector, exact (reference cu_freal<PB>::from_double, cu_freal.cuh:141-149) */
 int mpb_from_double(int prec, size_t n, const double *d, void *vec, void *stream);
 /* vector -> double[n], RNDN (reference cu_freal<PB>::to_double, cu_freal.cuh:150-165) */

@@ -66,6 +66,10 @@ _SIGS = {
     "mpb_fmath_c": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
     "mpb_div_ui_r": ([_I, _S, _V, C.c_uint64, _V, _V], C.c_int),
     "mpb_const_r": ([_I, _I, _S, _V, _V], C.c_int),
+    "mpb_aos_to_mpfr": ([_I, _S, _V, _V], C.c_int),
+    "mpb_aos_from_mpfr": ([_I, _S, _V, _V], C.c_int),
+    "mpb_caos_to_mpc": ([_I, _S, _V, _V], C.c_int),
+    "mpb_caos_from_mpc": ([_I, _S, _V, _V], C.c_int),
     "mpb_binop_c": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
     "mpb_axpy_r": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
     "mpb_axpy_c": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
