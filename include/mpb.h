@@ -77,6 +77,20 @@ int mpb_unpack_aos(int prec, size_t n, const void *vec, void *aos, void *stream)
 /* AoS cu_fcomplex<prec>[n] <-> complex tiled vector (reference cu_fcomplex.cuh:98-113) */
 int mpb_cpack_aos(int prec, size_t n, const void *aos, void *cvec, void *stream);
 int mpb_cunpack_aos(int prec, size_t n, const void *cvec, void *aos, void *stream);
+/* ---- arithmetic at a runtime precision (the hook for the reference's
+ * runtime-precision layer, src/mpfr_cuda/mpfr.h:582-589, 804: cu_mpfr_add /
+ * sub / mul / div / sqrt / fma with RNDN at the destination's precision) ----
+ * A precision prec (1 .. 2046 bits) is stored in the vector format of
+ * mpb_storage_prec(prec), the smallest supported PB >= prec + 2.  r[i] =
+ * op(a[i], b[i], c[i]) correctly rounded to nearest at prec bits (rounded to
+ * odd at PB bits, then to nearest at prec: exact by Boldo and Melquiond's
+ * theorem); operands may carry up to PB bits, results carry prec.  b is read
+ * unless op is MPB_RP_SQRT, c only for MPB_RP_FMA.  a / 0 and sqrt(a < 0)
+ * give 0. */
+enum { MPB_RP_MUL = 0, MPB_RP_ADD = 1, MPB_RP_SUB = 2, MPB_RP_FMA = 3, MPB_RP_DIV = 4, MPB_RP_SQRT = 5 };
+int mpb_storage_prec(int prec); /* PB, or MPB_ERR_PREC */
+int mpb_op_rp(int op, int prec, size_t n, const void *a, const void *b, const void *c, void *r, void *stream);
+
 /* ---- host interop with MPFR / MPC objects (host memory, no GPU, no MPFR link) ----
  * dst[i] / src[i] point to initialised mpfr_t (mpfr_ptr) or mpc_t objects; AoS
  * arrays are cu_freal<prec> / cu_fcomplex<prec> in host memory.  To MPFR: the

@@ -246,8 +246,18 @@ MPB_HD uint32_t inc_n(uint32_t *m, uint32_t inc) {
 
 /* Round-to-nearest-even increment of the NM-limb mantissa m given the round
  * bit rb and a nonzero-if-sticky word st; renormalises on carry-out. */
-template <int NM>
+/* round the mantissa m given the round bit rb and the sticky word st: to
+ * nearest-even (kRnd = 0), or to odd (kRnd = 1: truncate, then set the last
+ * bit when anything was lost -- the intermediate rounding that makes a later
+ * rounding to nearest at 2 or more bits fewer correct, Boldo and Melquiond,
+ * "Emulation of FMA and correctly rounded sums: proved algorithms using
+ * rounding to odd", IEEE Trans. Computers 2008) */
+template <int NM, int kRnd = 0>
 MPB_HD void rndn(uint32_t *m, int32_t &e, uint32_t rb, uint32_t st) {
+  if (kRnd == 1) {
+    m[0] |= (rb | st) != 0u ? 1u : 0u;
+    return;
+  }
   const uint32_t inc = rb & ((st != 0u) | (m[0] & 1u));
   const uint32_t c = inc_n<NM>(m, inc);
   m[NM - 1] |= c << 31; /* all-ones + 1 -> 1000...0 */
@@ -259,7 +269,7 @@ MPB_HD void rndn(uint32_t *m, int32_t &e, uint32_t rb, uint32_t st) {
  * ------------------------------------------------------------------ */
 /* Round an exact normalised-or-half-normalised 2N-limb product p (leading
  * one at bit 64N-1 or 64N-2) with exponent e (for the 64N-1 case) to N limbs. */
-template <int N>
+template <int N, int kRnd = 0>
 MPB_HD void round_prod(fval<N> &r, const uint32_t *p, int32_t e, uint32_t s) {
   const uint32_t sh = (p[2 * N - 1] >> 31) ^ 1u;
   MPB_UNROLL
@@ -270,7 +280,7 @@ MPB_HD void round_prod(fval<N> &r, const uint32_t *p, int32_t e, uint32_t s) {
   MPB_UNROLL
   for (int i = 0; i < N - 1; ++i) st |= p[i];
   r.e = e - (int32_t)sh;
-  rndn<N>(r.m, r.e, low >> 31, st);
+  rndn<N, kRnd>(r.m, r.e, low >> 31, st);
   r.s = s;
 }
 
@@ -312,11 +322,11 @@ MPB_HD void mul_high(uint32_t *p, const uint32_t *a, const uint32_t *b) {
 }
 
 /* the full product and its rounding, out of line: the rare case of mul */
-template <int N>
+template <int N, int kRnd = 0>
 MPB_NOINLINE void mul_full_round(fval<N> &r, const fval<N> &a, const uint32_t *bm, int32_t be, uint32_t bs) {
   uint32_t p[2 * N];
   mul_full<N>(p, a.m, bm);
-  round_prod<N>(r, p, a.e + be, a.s ^ bs);
+  round_prod<N, kRnd>(r, p, a.e + be, a.s ^ bs);
 }
 
 /* r = round(a * b), b given by its limbs (which may live in shared memory:
@@ -327,10 +337,12 @@ MPB_NOINLINE void mul_full_round(fval<N> &r, const fval<N> &a, const uint32_t *b
  * rounds down and X > 2^63 rounds up (a carry into the mantissa gives the
  * same result) whatever lambda is.  X in between -- about 2^-25 of random
  * operands, exact ties included -- rounds the full product instead. */
-template <int N>
+template <int N, int kRnd = 0>
 MPB_HD void mul_limbs(fval<N> &r, const fval<N> &a, const uint32_t *bm, int32_t be, uint32_t bs) {
   uint32_t p[2 * N];
-  if (N >= 4) {
+  if (kRnd == 1) { /* rounding to odd needs exactness: the full product */
+    mul_full_round<N, 1>(r, a, bm, be, bs);
+  } else if (N >= 4) {
     mul_high<N>(p, a.m, bm);
     MPB_UNROLL
     for (int i = 0; i < N - 2; ++i) p[i] = 0u;
@@ -348,9 +360,9 @@ MPB_HD void mul_limbs(fval<N> &r, const fval<N> &a, const uint32_t *bm, int32_t 
   if (is_zero(a) || be == kExpZero) set_zero(r);
 }
 /* the same with b as a value */
-template <int N>
+template <int N, int kRnd = 0>
 MPB_HD void mul(fval<N> &r, const fval<N> &a, const fval<N> &b) {
-  mul_limbs<N>(r, a, b.m, b.e, b.s);
+  mul_limbs<N, kRnd>(r, a, b.m, b.e, b.s);
 }
 
 /* exact product, normalised so that bit 31 of p[2N-1] is set (zero stays 0) */
@@ -392,7 +404,7 @@ struct log2_ceil<1> {
  * error must stay under a quarter ULP of r and the bits under the mantissa,
  * read as the 64-bit fraction G, clear of the midpoint by more than it (a
  * zero sum never certifies).  Without it the return value is true. */
-template <int NX, int NM, bool kVote = false, int kCertBits = 0>
+template <int NX, int NM, bool kVote = false, int kCertBits = 0, int kRnd = 0>
 MPB_HD bool add_round(fval<NM> &r, const uint32_t *xm, int32_t xe, uint32_t xs,
                       const uint32_t *ym, int32_t ye, uint32_t ys) {
   constexpr int W = NX + 2;
@@ -511,7 +523,7 @@ MPB_HD bool add_round(fval<NM> &r, const uint32_t *xm, int32_t xe, uint32_t xs,
     const uint64_t half = 1ull << 63;
     ok = !zero && t <= -3 && (G <= half - thr - 1 || G > half + thr);
   }
-  rndn<NM>(r.m, e, g >> 31, st);
+  rndn<NM, kRnd>(r.m, e, g >> 31, st);
   r.e = e;
   r.s = s;
   if (zero) set_zero(r);
@@ -519,17 +531,17 @@ MPB_HD bool add_round(fval<NM> &r, const uint32_t *xm, int32_t xe, uint32_t xs,
 }
 
 /* r = round(x + y), r = round(x - y) */
-template <int N, bool kVote = false>
+template <int N, bool kVote = false, int kRnd = 0>
 MPB_HD void add(fval<N> &r, const fval<N> &x, const fval<N> &y) {
-  add_round<N, N, kVote>(r, x.m, x.e, x.s, y.m, y.e, y.s);
+  add_round<N, N, kVote, 0, kRnd>(r, x.m, x.e, x.s, y.m, y.e, y.s);
 }
-template <int N, bool kVote = false>
+template <int N, bool kVote = false, int kRnd = 0>
 MPB_HD void sub(fval<N> &r, const fval<N> &x, const fval<N> &y) {
-  add_round<N, N, kVote>(r, x.m, x.e, x.s, y.m, y.e, y.s ^ (is_zero(y) ? 0u : 1u));
+  add_round<N, N, kVote, 0, kRnd>(r, x.m, x.e, x.s, y.m, y.e, y.s ^ (is_zero(y) ? 0u : 1u));
 }
 
 /* r = round(a*b + c), one rounding (MPFR mpfr_fma semantics) */
-template <int N, bool kVote = false>
+template <int N, bool kVote = false, int kRnd = 0>
 MPB_HD void fma(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c) {
   uint32_t p[2 * N], cw[2 * N];
   int32_t pe;
@@ -539,7 +551,7 @@ MPB_HD void fma(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c
     cw[i] = 0u;
     cw[N + i] = c.m[i];
   }
-  add_round<2 * N, N, kVote>(r, p, pe, a.s ^ b.s, cw, c.e, c.s);
+  add_round<2 * N, N, kVote, 0, kRnd>(r, p, pe, a.s ^ b.s, cw, c.e, c.s);
 }
 
 /* round(a*b - c*d) and round(a*b + c*d), one rounding each (MPFR
@@ -892,7 +904,7 @@ MPB_HD void divmod_limbs(uint32_t *q, uint32_t *u, const uint32_t *v) {
  * are the result, the next bit the round bit, the rest plus a nonzero
  * remainder the sticky bit.  b = 0 has no result in this format (no
  * infinities): r is 0. */
-template <int N>
+template <int N, int kRnd = 0>
 MPB_HD void div(fval<N> &r, const fval<N> &a, const fval<N> &b) {
   if (is_zero(a) || is_zero(b)) { /* no integer division by a zero divisor */
     set_zero(r);
@@ -911,7 +923,7 @@ MPB_HD void div(fval<N> &r, const fval<N> &a, const fval<N> &b) {
   const uint32_t rb = big ? (q[1] & 1u) : (q[0] >> 31);
   const uint32_t st = (big ? q[0] : (q[0] << 1)) | rem;
   int32_t e = a.e - b.e + (int32_t)big;
-  rndn<N>(r.m, e, rb, st);
+  rndn<N, kRnd>(r.m, e, rb, st);
   r.e = e;
   r.s = a.s ^ b.s;
 }
@@ -924,7 +936,7 @@ MPB_HD void div(fval<N> &r, const fval<N> &a, const fval<N> &b) {
  * 64 bits; it decreases to S and stops when it no longer decreases.  The top
  * 32N bits of S are the result, the next the round bit, the rest plus
  * S^2 != X the sticky bit.  Negative a has no result in this format: r is 0. */
-template <int N>
+template <int N, int kRnd = 0>
 MPB_HD void sqrt_(fval<N> &r, const fval<N> &a) {
   constexpr int NX = 2 * N + 2, NS = N + 1;
   if (is_zero(a) || a.s) { /* the iteration below needs a nonzero root */
@@ -982,7 +994,7 @@ MPB_HD void sqrt_(fval<N> &r, const fval<N> &a) {
   const uint32_t rb = s[0] >> 31;
   const uint32_t st = (s[0] << 1) | diff;
   int32_t e = (a.e + (int32_t)odd) >> 1; /* e/2 (E even) or (e+1)/2 (E odd), exactly */
-  rndn<N>(r.m, e, rb, st);
+  rndn<N, kRnd>(r.m, e, rb, st);
   r.e = e;
   r.s = 0u;
 }

@@ -66,6 +66,8 @@ _SIGS = {
     "mpb_fmath_c": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
     "mpb_div_ui_r": ([_I, _S, _V, C.c_uint64, _V, _V], C.c_int),
     "mpb_const_r": ([_I, _I, _S, _V, _V], C.c_int),
+    "mpb_storage_prec": ([_I], C.c_int),
+    "mpb_op_rp": ([_I, _I, _S, _V, _V, _V, _V, _V], C.c_int),
     "mpb_aos_to_mpfr": ([_I, _S, _V, _V], C.c_int),
     "mpb_aos_from_mpfr": ([_I, _S, _V, _V], C.c_int),
     "mpb_caos_to_mpc": ([_I, _S, _V, _V], C.c_int),
@@ -141,6 +143,7 @@ def host_lib():
             getattr(H, name).argtypes = [_I, _I, _L, _V, _V, _V]
         H.mpbh_div_ui.argtypes = [_I, _L, _V, C.c_ulonglong, _V]
         H.mpbh_const.argtypes = [_I, _I, _V]
+        H.mpbh_op_rp.argtypes = [_I, _I, _L, _V, _V, _V, _V]
         for name in ("mpbh_axpy_r", "mpbh_axpy_c"):
             getattr(H, name).argtypes = [_I, _L, _V, _V, _V, _V]
         H.mpbh_from_double.argtypes = [_I, _L, _V, _V]
@@ -267,6 +270,23 @@ def div_ui(prec, n, a, u, r, stream=None):
 def const(which, prec, n, r, stream=None):
     """r[0 .. n) = pi ('pi') or ln 2 ('ln2'), correctly rounded (cu_pi / cu_ln2)."""
     _call("mpb_const_r", 0 if which == "pi" else 1, prec, n, _ptr(r), _stream(stream))
+
+
+RP_OPS = ("mul", "add", "sub", "fma", "div", "sqrt")
+
+
+def storage_prec(prec):
+    """the supported PB whose vectors hold precision prec (PB >= prec + 2)"""
+    pb = lib().mpb_storage_prec(prec)
+    if pb < 0:
+        raise MpbError(pb, "mpb_storage_prec")
+    return pb
+
+
+def op_rp(op, prec, n, a, r, b=None, c=None, stream=None):
+    """r = op(a, b, c) correctly rounded at a runtime precision prec (vectors in
+    the storage_prec(prec) format); op in RP_OPS."""
+    _call("mpb_op_rp", RP_OPS.index(op), prec, n, _ptr(a), _ptr(b), _ptr(c), _ptr(r), _stream(stream))
 
 
 def fma(prec, n, a, b, c, r, cplx=False, stream=None):

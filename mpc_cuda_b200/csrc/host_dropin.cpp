@@ -22,13 +22,17 @@
  *                                        b only for the division)
  *   mpbh_div_ui(prec, n, a, u, r)        cu_div_ui
  *   mpbh_const(which, prec, r)           cu_pi (0) / cu_ln2 (1)
+ *   mpbh_op_rp(op, p, n, a, b, c, r)     op at a runtime precision p (mpb.h
+ *                                        MPB_RP_*), AoS of the storage PB
  *   mpbh_axpy_r / mpbh_axpy_c(prec, n, a, x, y, z)
  *   mpbh_from_double / mpbh_to_double(prec, n, ...)
  * Return 0, or -1 for an unsupported precision.
  */
 #include <cstdint>
+#include <initializer_list>
 
 #include "mpc_cuda.cuh"
+#include "mpb/rprec.cuh"
 
 using cu_fp::cu_fcomplex;
 using cu_fp::cu_freal;
@@ -138,6 +142,23 @@ void const1(int which, void *R) {
   *(cu_freal<PB> *)R = which == 0 ? cu_fp::cu_pi<PB>() : cu_fp::cu_ln2<PB>();
 }
 template <int PB>
+void op_rp1(int op, int p, long n, const void *A, const void *B, const void *Cc, void *R) {
+  typedef typename cu_fp::detail::core_of<PB>::type F;
+  auto a = (const cu_freal<PB> *)A;
+  auto b = (const cu_freal<PB> *)B;
+  auto c = (const cu_freal<PB> *)Cc;
+  auto r = (cu_freal<PB> *)R;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    F x, y, z, o;
+    cu_fp::detail::to_core<PB>(x, a[i]);
+    cu_fp::detail::to_core<PB>(y, op == 5 ? a[i] : b[i]);
+    cu_fp::detail::to_core<PB>(z, op == 3 ? c[i] : a[i]);
+    mpb::op_rp(op, p, o, x, y, z);
+    r[i] = cu_fp::detail::from_core<PB>(o);
+  }
+}
+template <int PB>
 void cfma3(long n, const void *A, const void *B, const void *C, void *R) {
   auto a = (const cu_fcomplex<PB> *)A;
   auto b = (const cu_fcomplex<PB> *)B;
@@ -238,6 +259,14 @@ int mpbh_div_ui(int prec, long n, const void *a, unsigned long long u, void *r) 
   MPBH_DISPATCH(prec, div_ui1<PB>(n, a, u, r))
 }
 int mpbh_const(int which, int prec, void *r) { MPBH_DISPATCH(prec, const1<PB>(which, r)) }
+int mpbh_op_rp(int op, int p, long n, const void *a, const void *b, const void *c, void *r) {
+  if (op < 0 || op > 5 || p < 1) return -2;
+  int pb = 0;
+  for (int q : {64, 128, 256, 512, 1024, 2048})
+    if (!pb && q >= p + 2) pb = q;
+  if (!pb) return -1;
+  MPBH_DISPATCH(pb, op_rp1<PB>(op, p, n, a, b, c, r))
+}
 int mpbh_cfma(int prec, long n, const void *a, const void *b, const void *c, void *r) {
   MPBH_DISPATCH(prec, cfma3<PB>(n, a, b, c, r))
 }

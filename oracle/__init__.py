@@ -62,6 +62,7 @@ def lib():
             getattr(L, name).argtypes = [it, it, it, lg, vp, vp, vp]
         L.mp_div_ui.argtypes = [it, lg, vp, C.c_ulong, vp]
         L.mp_const.argtypes = [it, it, vp]
+        L.mp_op_rp.argtypes = [it, it, it, lg, vp, vp, vp, vp]
         for name in ("orc_fma", "mp_fma", "mp_cfma", "mp_cfma_dot"):
             getattr(L, name).argtypes = [it, lg, vp, vp, vp, vp]
         for name in ("orc_axpy_r", "orc_axpy_c", "mp_axpy_r", "mp_axpy_c"):
@@ -278,6 +279,15 @@ def div_ui(prec: int, A, u: int) -> np.ndarray:
     """round(a / u), mpfr_div_ui (RNDN)."""
     R = empty(prec, A.shape[0])
     lib().mp_div_ui(prec, A.shape[0], _p(A), u, _p(R))
+    return R
+
+
+def op_rp(op: str, p: int, P: int, A, B=None, Cc=None) -> np.ndarray:
+    """op (mul, add, sub, fma, div, sqrt) rounded to nearest at p bits by the
+    system MPFR, operands and results in the P-bit element format."""
+    R = empty(P, A.shape[0])
+    lib().mp_op_rp(("mul", "add", "sub", "fma", "div", "sqrt").index(op), p, P, A.shape[0], _p(A), _p(B), _p(Cc),
+                   _p(R))
     return R
 
 

@@ -1019,6 +1019,46 @@ int mp_fn(int fn, int P, int Pout, long n, const void *A, const void *B, void *R
   return 0;
 }
 
+/* a p-bit MPFR value into a P-bit element (p <= P): the significand in the
+ * top limbs, zeros below */
+static void store_mpfr_narrow(int P, elem_t *e, const shim_mpfr_struct *x) {
+  if (mpfr_zero_p(x)) {
+    set_zero(P, e);
+    return;
+  }
+  int n = n64_of(P), nx = (int)((x->prec + 63) / 64);
+  memset(e->m, 0, 8 * (size_t)n);
+  memcpy(e->m + (n - nx), x->d, 8 * (size_t)nx);
+  e->sign = x->sign < 0 ? -1 : 1;
+  e->pad = 0;
+  e->exp = x->exp;
+}
+
+/* op(a, b, c) rounded to nearest at precision p, operands and result in the
+ * P-bit element format (op 0 mul, 1 add, 2 sub, 3 fma, 4 div, 5 sqrt): the
+ * checker for the engine's runtime-precision arithmetic */
+void mp_op_rp(int op, int p, int P, long n, const void *A, const void *B, const void *C, void *R) {
+  size_t es = esz_of(P);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    shim_mpfr_t a, b, c, r;
+    as_mpfr(P, a, cat(A, es, i));
+    as_mpfr(P, b, cat(op == 5 ? A : B, es, i));
+    as_mpfr(P, c, cat(op == 3 ? C : A, es, i));
+    mpfr_init2(r, p);
+    switch (op) {
+      case 0: mpfr_mul(r, a, b, SHIM_RNDN); break;
+      case 1: mpfr_add(r, a, b, SHIM_RNDN); break;
+      case 2: mpfr_sub(r, a, b, SHIM_RNDN); break;
+      case 3: mpfr_fma(r, a, b, c, SHIM_RNDN); break;
+      case 4: mpfr_div(r, a, b, SHIM_RNDN); break;
+      default: mpfr_sqrt(r, a, SHIM_RNDN);
+    }
+    store_mpfr_narrow(P, at(R, es, i), r);
+    mpfr_clear(r);
+  }
+}
+
 /* round(a / u) (mpfr_div_ui), and pi / ln 2 (which 0 / 1) at precision P */
 void mp_div_ui(int P, long n, const void *A, unsigned long u, void *R) {
   size_t es = esz_of(P);

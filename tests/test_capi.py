@@ -58,6 +58,18 @@ def test_bad_arguments_rejected_on_host(mpb):
     assert L.mpb_gemv_r(256, 4, 50, good, 32, good, good, good, None) == -5
     # size overflow
     assert L.mpb_axpy_r(256, 1 << 62, good, good, good, good, None) == -2
+    # elementary functions: unknown function, missing second operand
+    assert L.mpb_fmath_r(16, 256, 10, good, None, good, None) == -7
+    assert L.mpb_fmath_r(14, 256, 10, good, None, good, None) == -3  # pow needs b
+    assert L.mpb_fmath_c(9, 256, 10, good, good, good, None) == -7
+    assert L.mpb_fmath_c(8, 256, 10, good, None, good, None) == -3  # division needs b
+    assert L.mpb_const_r(2, 256, 10, good, None) == -7
+    assert L.mpb_div_ui_r(100, 10, good, 3, good, None) == -1
+    # runtime precision: storage formats and bad arguments
+    assert [L.mpb_storage_prec(p) for p in (1, 62, 63, 126, 127, 2046, 2047, 0)] == [64, 64, 128, 128, 256, 2048, -1, -1]
+    assert L.mpb_op_rp(6, 100, 10, good, good, good, good, None) == -7
+    assert L.mpb_op_rp(0, 2047, 10, good, good, good, good, None) == -1
+    assert L.mpb_op_rp(3, 100, 10, good, good, None, good, None) == -3  # fma needs c
 
 
 def test_empty_inputs_are_noops(mpb):
@@ -67,6 +79,8 @@ def test_empty_inputs_are_noops(mpb):
     assert L.mpb_gemm_r(512, 0, 8, 8, None, 32, None, 32, None, 32, None) == 0
     assert L.mpb_gemv_c(256, 0, 5, None, 32, None, None, None, None) == 0
     assert L.mpb_pack_aos(256, 0, None, None, None) == 0
+    assert L.mpb_fmath_r(0, 256, 0, None, None, None, None) == 0
+    assert L.mpb_op_rp(0, 100, 0, None, None, None, None, None) == 0
 
 
 def test_exact_gemm_workspace_and_checks(mpb):

@@ -382,3 +382,21 @@ def test_div_ui_and_constants(orc, mpb, prec):
         mpb.const(which, prec, 40, r)
         want = np.repeat(orc.const(which, prec), 40, axis=0)
         assert orc.mismatches(prec, hvec(prec, r, 40), want)[0] == 0, which
+
+
+@pytest.mark.parametrize("p", (2, 53, 63, 113, 200, 255, 300, 511, 1000, 1023, 2046))
+def test_runtime_precision_ops(orc, mpb, p):
+    """mpb_op_rp: every operation at precision p bit-identical to MPFR with a
+    p-bit destination (storage format PB = mpb_storage_prec(p))."""
+    from test_host_dropin import rp_operands
+
+    n = 4000 if p <= 1023 else 1000
+    pb, A, Apos, B, Cc = rp_operands(orc, p, n, 0x9100 + p)
+    assert mpb.storage_prec(p) == pb
+    b, c = dvec(pb, B), dvec(pb, Cc)
+    for op in mpb.RP_OPS:
+        X = Apos if op == "sqrt" else A
+        r = mpb.empty(pb, n)
+        mpb.op_rp(op, p, n, dvec(pb, X), r, b=b, c=c)
+        bad, first = orc.mismatches(pb, hvec(pb, r, n), orc.op_rp(op, p, pb, X, B, Cc))
+        assert bad == 0, f"{op} p={p}: {bad} mismatches, first at {first}"

@@ -399,3 +399,38 @@ def test_div_ui_and_constants(orc, mpb, prec):
         R = orc.empty(prec, 1)
         assert H.mpbh_const(k, prec, _p(R)) == 0
         assert orc.mismatches(prec, R, orc.const(which, prec))[0] == 0, which
+
+
+# ---------------------------------------------------------------- runtime precision
+RP_PRECS = (1, 2, 24, 53, 62, 63, 100, 113, 126, 127, 200, 254, 255, 300, 510, 511, 1000, 1022, 1023, 1500, 2046)
+
+
+def rp_storage(p):
+    return next(q for q in (64, 128, 256, 512, 1024, 2048) if q >= p + 2)
+
+
+def rp_operands(orc, p, n, seed):
+    """operands in the storage format: the reference's pairs (exponent spreads
+    40 and PB+200) plus a third operand; sqrt gets |a|"""
+    pb = rp_storage(p)
+    A, B = orc.gen_pairs(pb, n, seed)
+    Cc, _ = orc.gen_pairs(pb, n, seed + 1)
+    Apos = A.copy()
+    Apos[:, 0:4] = np.array([1], np.int32).view(np.uint8)
+    return pb, A, Apos, B, Cc
+
+
+@pytest.mark.parametrize("p", RP_PRECS)
+def test_runtime_precision_ops(orc, mpb, p):
+    """mul / add / sub / fma / div / sqrt at any precision p (rounded to odd
+    at the storage PB, then to nearest at p): bit-identical to MPFR with a
+    p-bit destination (the reference's runtime layer, mpfr_cuda/mpfr.h:582-589)."""
+    H = mpb.host_lib()
+    n = 1500 if p <= 1023 else 400
+    pb, A, Apos, B, Cc = rp_operands(orc, p, n, 0x9000 + p)
+    for k, op in enumerate(("mul", "add", "sub", "fma", "div", "sqrt")):
+        X = Apos if op == "sqrt" else A
+        R = orc.empty(pb, n)
+        assert H.mpbh_op_rp(k, p, n, _p(X), _p(B), _p(Cc), _p(R)) == 0
+        bad, first = orc.mismatches(pb, R, orc.op_rp(op, p, pb, X, B, Cc))
+        assert bad == 0, f"{op} p={p}: {bad} mismatches, first at {first}"
