@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpb|reference]
                     [--workload gemm_r512|gemm_c256|gemv_batch|axpy_c1024|axpy_r256|
-                                div_r512|sqrt_r512|exp_r512|log_r512|sin_r512]
+                                div_r512|sqrt_r512|exp_r512|log_r512|sin_r512|cexp_c512]
 
 One JSON line on stdout (rank 0).  A step is one pass of the hot path over
 one batch of synthetic operands already resident in HBM; K steps are timed
@@ -731,7 +731,79 @@ class DivSqrtWorkload(AxpyWorkload):
                 "l2": f"{self.nsets} rotating input sets > L2"}
 
 
+class CfnWorkload(AxpyWorkload):
+    """z = c<op>(x) over n complex elements at precision prec (each component
+    faithful, the contract of the reference's cu_cexp); the CPU baseline is
+    the reference's own cu_fcmath function built for the host."""
+
+    def __init__(self, name, op, prec, n, seed):
+        super().__init__(name, True, prec, n, seed)
+        self.op = op
+        self.metric = f"faithful complex {op} (c{op}) per second at PB={prec}"
+        self.unit = f"mp-c{op}/s"
+        self.desc = (f"complex {op} z=c{op}(x), cu_fcomplex<{prec}>, each component faithful, "
+                     f"n=2^{n.bit_length() - 1}, full random significands, component exponents in [-3, 3]")
+
+    @property
+    def default_steps(self):  # about 1 s of GPU time
+        return 100
+
+    def make_host(self, rank):
+        from mpc_cuda_b200 import synth
+
+        rng = np.random.default_rng(self.seed + 1000 * rank)
+        re = synth.random_elems(rng, self.prec, self.n, -3, 3)
+        im = synth.random_elems(rng, self.prec, self.n, -3, 3)
+        x = synth.interleave_complex(self.prec, re, im)
+        return x[:1], x, x  # one input: the AXPY plumbing's a and y go unused
+
+    def step(self, i, stream):
+        x, _, z = self.sets[i % self.nsets]
+        self.M.cfmath(self.op, self.prec, self.n, x, z, stream=stream)
+
+    def e2e_h2d(self, s):
+        self.dx_aos[s].copy_(self.hx, non_blocking=True)
+
+    def e2e_bytes(self):
+        return self.host[1].size, self.host[1].size
+
+    e2e_launches_per_step = 3
+
+    def e2e_compute(self, s, stream):
+        M = self.M
+        M.pack_aos(self.prec, self.n, self.dx_aos[s], self.ex, True, stream=stream)
+        M.cfmath(self.op, self.prec, self.n, self.ex, self.ez, stream=stream)
+        M.unpack_aos(self.prec, self.n, self.ez, self.dz_aos[s], True, stream=stream)
+
+    def roofline(self, kernel_s, peaks, imad_ops_s):
+        NW = self.prec // 32 + 4
+        s_e, T_e, s_c, T_c, _ = _elem_params(NW)
+        mulw, dui = rounded_product_imads(NW), 5 * (NW + 2)
+        # cexp: the exponential of the real part, sine and cosine of the
+        # imaginary part (the two series and the doublings), two products --
+        # estimated from the implemented algorithms, as for the real functions
+        per = ((T_e - 1) * (mulw + dui) + (2 + s_e) * mulw + 2 * T_c * (mulw + dui) + 3 * mulw
+               + 2 * s_c * mulw + 2 * mulw)
+        imad = per * self.n / kernel_s
+        return {"bound": "imad", "achieved": round(imad / 1e9, 1),
+                "peak": round(imad_ops_s / 1e9, 1) if imad_ops_s else None, "unit": "Gop/s",
+                "frac": round(imad / imad_ops_s, 4) if imad_ops_s else None, "ops_per_unit": per,
+                "peak_source": "libmpb_probe.so mad.lo/mad.hi throughput, measured in this run", "traffic": None}
+
+    def cpu_run(self, impl, count):
+        import oracle as O
+
+        O.cfn(self.op, self.prec, self.host[1][:count], impl="ref" if impl == "ref" else "mp")
+        return count
+
+    def config(self):
+        return {"workload": self.desc, "prec": self.prec, "n": self.n,
+                "units": f"one faithful complex {self.op} (both components)",
+                "l2": f"{self.nsets} rotating input sets > L2"}
+
+
 WORKLOADS = {
+    "cexp_c512": lambda: CfnWorkload("cexp_c512", "exp", 512, 1 << 18, 0x5EEDB),
     "div_r512": lambda: DivSqrtWorkload("div_r512", "div", 512, 1 << 20, 0x5EED6),
     "sqrt_r512": lambda: DivSqrtWorkload("sqrt_r512", "sqrt", 512, 1 << 20, 0x5EED7),
     "exp_r512": lambda: DivSqrtWorkload("exp_r512", "exp", 512, 1 << 18, 0x5EED8),
