@@ -321,12 +321,39 @@ MPB_HD void mul_high(uint32_t *p, const uint32_t *a, const uint32_t *b) {
   p[2 * N - 1] = c0;
 }
 
-/* the full product and its rounding, out of line: the rare case of mul */
+/* the full product and its rounding, out of line: the rare case of mul.
+ * Up to kByValueLimbs limbs the operands and the result travel by value: the
+ * call passes them in registers, whereas references to a caller's registers
+ * make the caller keep those values in local memory (a stack frame) for the
+ * call.  Above it the argument registers run out and by-value passing spills,
+ * so wider operands go by reference. */
+constexpr int kByValueLimbs = 20;
 template <int N, int kRnd = 0>
-MPB_NOINLINE void mul_full_round(fval<N> &r, const fval<N> &a, const uint32_t *bm, int32_t be, uint32_t bs) {
+MPB_NOINLINE fval<N> mul_full_round_v(fval<N> a, fval<N> b) {
+  uint32_t p[2 * N];
+  mul_full<N>(p, a.m, b.m);
+  fval<N> r;
+  round_prod<N, kRnd>(r, p, a.e + b.e, a.s ^ b.s);
+  return r;
+}
+template <int N, int kRnd = 0>
+MPB_NOINLINE void mul_full_round_r(fval<N> &r, const fval<N> &a, const uint32_t *bm, int32_t be, uint32_t bs) {
   uint32_t p[2 * N];
   mul_full<N>(p, a.m, bm);
   round_prod<N, kRnd>(r, p, a.e + be, a.s ^ bs);
+}
+template <int N, int kRnd = 0>
+MPB_HD void mul_full_round(fval<N> &r, const fval<N> &a, const uint32_t *bm, int32_t be, uint32_t bs) {
+  if constexpr (N <= kByValueLimbs) {
+    fval<N> b;
+    MPB_UNROLL
+    for (int i = 0; i < N; ++i) b.m[i] = bm[i];
+    b.e = be;
+    b.s = bs;
+    r = mul_full_round_v<N, kRnd>(a, b);
+  } else {
+    mul_full_round_r<N, kRnd>(r, a, bm, be, bs);
+  }
 }
 
 /* r = round(a * b), b given by its limbs (which may live in shared memory:
@@ -558,13 +585,31 @@ MPB_HD void fma(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c
  * mpfr_fmms / mpfr_fmma semantics; the exact-intermediate complex product
  * of MPC_RNDNN, mpc_cuda cu_fcomplex.cuh:91-96) */
 template <int N>
-MPB_NOINLINE void fmms_full(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c, const fval<N> &d,
-                            uint32_t negate_cd) {
+MPB_NOINLINE fval<N> fmms_full_v(fval<N> a, fval<N> b, fval<N> c, fval<N> d, uint32_t negate_cd) {
+  uint32_t p1[2 * N], p2[2 * N];
+  int32_t e1, e2;
+  mul_exact_norm<N>(p1, e1, a, b);
+  mul_exact_norm<N>(p2, e2, c, d);
+  fval<N> r;
+  add_round<2 * N, N>(r, p1, e1, a.s ^ b.s, p2, e2, c.s ^ d.s ^ negate_cd);
+  return r;
+}
+template <int N>
+MPB_NOINLINE void fmms_full_r(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c, const fval<N> &d,
+                              uint32_t negate_cd) {
   uint32_t p1[2 * N], p2[2 * N];
   int32_t e1, e2;
   mul_exact_norm<N>(p1, e1, a, b);
   mul_exact_norm<N>(p2, e2, c, d);
   add_round<2 * N, N>(r, p1, e1, a.s ^ b.s, p2, e2, c.s ^ d.s ^ negate_cd);
+}
+template <int N>
+MPB_HD void fmms_full(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c, const fval<N> &d,
+                      uint32_t negate_cd) {
+  if constexpr (N <= kByValueLimbs)
+    r = fmms_full_v<N>(a, b, c, d, negate_cd);
+  else
+    fmms_full_r<N>(r, a, b, c, d, negate_cd);
 }
 
 /* upper columns of a*b (mul_high), normalised like mul_exact_norm; zero stays 0 */

@@ -27,27 +27,27 @@ struct cu_wterm {
   cu_limb M[WN];
 };
 
-/* exact a*b as a wide term (reference cu_mk_term, cu_fcomplex.cuh:30-42) */
+/* exact a*b as a wide term (reference cu_mk_term, cu_fcomplex.cuh:30-42): the
+ * core's exact normalised product of the two 32-bit-word significands, whose
+ * 2 PB/32 words fill the term's 64-bit limbs from the top */
 template <int PB>
 __host__ __device__ static cu_wterm<PB> cu_mk_term(const cu_freal<PB> &a, const cu_freal<PB> &b) {
+  typedef detail::core_of<PB> Cr;
+  const int WN = cu_wterm<PB>::WN, NP = 2 * Cr::N32, OFF = 2 * WN - NP; /* zero low halves */
+  typename Cr::type x, y;
+  detail::to_core<PB>(x, a);
+  detail::to_core<PB>(y, b);
+  uint32_t p[NP];
+  int32_t e;
+  mpb::mul_exact_norm<Cr::N32>(p, e, x, y);
   cu_wterm<PB> t;
-  const int WN = cu_wterm<PB>::WN;
-  if (a.is_zero() || b.is_zero()) {
-    t.zero = true;
-    t.sign = 1;
-    t.exp = 0;
-    for (int i = 0; i < WN; i++) t.M[i] = 0;
-    return t;
-  }
-  t.zero = false;
-  t.sign = a.sign * b.sign;
-  cu_mul_full<PB>(t.M, a.m, b.m);
-  if (t.M[WN - 1] >> 63) {
-    t.exp = a.exp + b.exp;
-  } else {
-    for (int i = WN - 1; i > 0; i--) t.M[i] = (t.M[i] << 1) | (t.M[i - 1] >> 63);
-    t.M[0] <<= 1;
-    t.exp = a.exp + b.exp - 1;
+  t.zero = a.is_zero() || b.is_zero();
+  t.sign = t.zero ? 1 : a.sign * b.sign;
+  t.exp = t.zero ? 0 : (long)e;
+  for (int k = 0; k < WN; k++) {
+    const int lo = 2 * k - OFF, hi = lo + 1;
+    const cu_limb l = (!t.zero && lo >= 0) ? p[lo] : 0u, h = (!t.zero && hi >= 0) ? p[hi] : 0u;
+    t.M[k] = (h << 32) | l;
   }
   return t;
 }

@@ -25,7 +25,7 @@
 #include <cmath>
 #include <cstdint>
 
-#include "../mpb/core.cuh"
+#include "../mpb/rprec.cuh"
 
 #if !defined(__CUDACC__)
 #ifndef __host__
@@ -52,21 +52,44 @@ __host__ __device__ static inline void cu_umul(cu_limb &hi, cu_limb &lo, cu_limb
   hi = (cu_limb)(p >> 64);
 #endif
 }
-/* bit i of W[len], 0 outside (reference cu_freal.cuh:52-54) */
+/* bit i of the little-endian limb array W[len]; bits outside it read as 0
+ * (reference cu_freal.cuh:52-54) */
 __host__ __device__ static inline cu_limb cu_wbit(const cu_limb *W, int len, long i) {
-  if (i < 0 || i >= (long)len * 64) return 0;
-  return (W[i >> 6] >> (i & 63)) & 1;
+  const unsigned long u = (unsigned long)i; /* negative i wraps to a huge index */
+  return u < 64ul * (unsigned long)len ? (W[u / 64] >> (u % 64)) & 1ull : 0ull;
 }
-/* 1 if any of bits [0, i) of W is set (reference cu_freal.cuh:56-64) */
+/* 1 when some bit of W below position i is set, else 0 (reference
+ * cu_freal.cuh:56-64): every limb is masked to the part of it that lies
+ * below i and the masked limbs are ORed */
 __host__ __device__ static inline cu_limb cu_wsticky_below(const cu_limb *W, int len, long i) {
-  if (i <= 0) return 0;
-  long full = i >> 6;
-  cu_limb s = 0;
-  for (long j = 0; j < full && j < len; j++) s |= W[j];
-  int rem = (int)(i & 63);
-  if (rem && full < len) s |= W[full] & ((((cu_limb)1) << rem) - 1);
-  return s != 0;
+  cu_limb any = 0;
+  for (int j = 0; j < len; j++) {
+    const long below = i - 64L * j; /* bits of limb j under position i */
+    if (below <= 0) break;
+    any |= below >= 64 ? W[j] : W[j] & ~(~0ull << below);
+  }
+  return any ? 1ull : 0ull;
 }
+
+template <int PB>
+struct cu_freal;
+
+namespace detail {
+/* limb i of D[len], 0 outside the array */
+__host__ __device__ inline cu_limb limb_or0(const cu_limb *D, int len, long i) {
+  return (i >= 0 && i < len) ? D[i] : 0ull;
+}
+/* the 32 bits [pos, pos + 32) of the magnitude D[len] (64-bit limbs); bits
+ * outside [0, 64 len) read as 0 */
+__host__ __device__ inline uint32_t dbits32(const cu_limb *D, int len, long pos) {
+  if (pos <= -32) return 0u;
+  if (pos < 0) return (uint32_t)(limb_or0(D, len, 0) << (-pos));
+  const long w = pos >> 6;
+  const int b = (int)(pos & 63);
+  const cu_limb lo = limb_or0(D, len, w), hi = limb_or0(D, len, w + 1);
+  return (uint32_t)(b ? (lo >> b) | (hi << (64 - b)) : lo);
+}
+}  // namespace detail
 
 template <int PB>
 struct cu_freal {
@@ -86,91 +109,22 @@ struct cu_freal {
     for (int i = 0; i < N; i++) m[i] = 0;
   }
 
-  /* Round the exact magnitude D[len] (leading one at bit msb, of weight 2^Ehi,
-   * with round/sticky material brnd/bsti strictly below bit 0) to P bits,
-   * RNDN (reference cu_freal.cuh:83-138).  General-purpose, used by the
-   * conversions; the arithmetic goes through the mpb core instead. */
-  __host__ __device__ static cu_freal finalize(const cu_limb *D, int len, int msb, long Ehi,
-                                               cu_limb brnd, cu_limb bsti, int sgn) {
-    cu_freal r;
-    if (msb < 0) {
-      r.set_zero();
-      return r;
-    }
-    const long lo = (long)msb - P + 1;
-    cu_limb V[N];
-    for (int i = 0; i < N; i++) { /* bits [lo + 64i, lo + 64i + 64) */
-      const long pos = lo + 64L * i;
-      const long w = pos >= 0 ? pos / 64 : -((-pos + 63) / 64);
-      const int b = (int)(pos - 64 * w);
-      const cu_limb a0 = (w >= 0 && w < len) ? D[w] : 0;
-      const cu_limb a1 = (w + 1 >= 0 && w + 1 < len) ? D[w + 1] : 0;
-      V[i] = b ? (a0 >> b) | (a1 << (64 - b)) : a0;
-    }
-    if (SB) V[N - 1] &= (((cu_limb)1) << (64 - SB)) - 1;
-    cu_limb rb = 0, st = 0;
-    if (lo > 0) {
-      rb = cu_wbit(D, len, lo - 1);
-      st = brnd | bsti | cu_wsticky_below(D, len, lo - 1);
-    } else if (lo == 0) {
-      rb = brnd;
-      st = bsti;
-    }
-    long E = Ehi;
-    if (rb && (st || (V[0] & 1))) {
-      cu_limb c = 1;
-      for (int i = 0; i < N && c; i++) {
-        V[i] += c;
-        c = (V[i] == 0);
-      }
-      const bool ov = SB ? (((V[N - 1] >> (64 - SB)) & 1) != 0) : (c != 0);
-      if (ov) {
-        for (int i = 0; i < N; i++) V[i] = 0;
-        V[(P - 1) >> 6] = ((cu_limb)1) << ((P - 1) & 63);
-        E++;
-      }
-    }
-    for (int i = N - 1; i >= 0; i--) {
-      const cu_limb hi = V[i], lo2 = (i > 0) ? V[i - 1] : 0;
-      r.m[i] = SB ? (hi << SB) | (lo2 >> (64 - SB)) : hi;
-    }
-    r.sign = sgn;
-    r.exp = E + 1;
-    return r;
-  }
+  /* Round a magnitude to PB bits, RNDN, and give it the sign sgn (the
+   * argument meaning of the reference's finalize, cu_freal.cuh:83-138):
+   * D[len] holds the significant bits (little-endian 64-bit limbs), its
+   * leading one at bit msb (msb < 0: the value is zero) with weight 2^Ehi,
+   * and brnd / bsti are the round bit and the sticky bit of what lies below
+   * D's bit 0 (used only when the result's last bit is at or above D's bit 0;
+   * a result with fewer than PB significant bits in D is exact).
+   * The PB bits under the leading one are read as PB/32 words of the mpb
+   * core, rounded there (mpb::rndn) and packed into the 64-bit limbs. */
+  __host__ __device__ static cu_freal finalize(const cu_limb *D, int len, int msb, long Ehi, cu_limb brnd,
+                                               cu_limb bsti, int sgn);
 
-  /* exact for PB >= 53 (reference cu_freal.cuh:141-149) */
-  __host__ __device__ static cu_freal from_double(double d) {
-    cu_freal r;
-    if (d == 0.0) {
-      r.set_zero();
-      return r;
-    }
-    const int sgn = d < 0 ? -1 : 1;
-    d = d < 0 ? -d : d;
-    int k;
-    const double f = frexp(d, &k);
-    cu_limb F = (cu_limb)ldexp(f, 53);
-    return finalize(&F, 1, 52, (long)k - 1, 0, 0, sgn);
-  }
+  /* exact for PB >= 53, rounded to PB bits below that (reference cu_freal.cuh:141-149) */
+  __host__ __device__ static cu_freal from_double(double d);
   /* RNDN to 53 bits (reference cu_freal.cuh:150-165) */
-  __host__ __device__ double to_double() const {
-    if (is_zero()) return 0.0;
-    const int hb = N * 64 - 53;
-    const int w = hb >> 6, b = hb & 63;
-    cu_limb F = b ? (m[w] >> b) | (w + 1 < N ? m[w + 1] << (64 - b) : 0) : m[w];
-    const cu_limb rbit = cu_wbit(m, N, hb - 1);
-    const cu_limb sticky = cu_wsticky_below(m, N, hb - 1);
-    long e = exp;
-    if (rbit && (sticky || (F & 1))) {
-      F++;
-      if (F == (1ULL << 53)) {
-        F >>= 1;
-        e++;
-      }
-    }
-    return (double)sign * ldexp((double)F, (int)(e - 53));
-  }
+  __host__ __device__ double to_double() const;
 
   __host__ __device__ cu_freal() {}
   __host__ __device__ cu_freal(double d) { *this = from_double(d); }
@@ -200,25 +154,129 @@ __host__ __device__ inline void to_core(typename core_of<PB>::type &r, const cu_
   r.e = (int32_t)x.exp;
   r.s = x.sign < 0 ? 1u : 0u;
 }
+/* the core words of r in the 64-bit limbs of x (the low SB bits stay 0) */
 template <int PB>
-__host__ __device__ inline cu_freal<PB> from_core(const typename core_of<PB>::type &r) {
+__host__ __device__ inline void pack_limbs(cu_freal<PB> &x, const typename core_of<PB>::type &r) {
   typedef core_of<PB> C;
-  cu_freal<PB> x;
-  if (mpb::is_zero(r)) {
-    x.set_zero();
-    return x;
-  }
   for (int k = 0; k < cu_freal<PB>::N; k++) {
     const int lo = 2 * k - C::OFF, hi = 2 * k + 1 - C::OFF;
     const cu_limb l = (lo >= 0 && lo < C::N32) ? r.m[lo] : 0u;
     const cu_limb h = (hi >= 0 && hi < C::N32) ? r.m[hi] : 0u;
     x.m[k] = (h << 32) | l;
   }
+}
+template <int PB>
+__host__ __device__ inline cu_freal<PB> from_core(const typename core_of<PB>::type &r) {
+  cu_freal<PB> x;
+  if (mpb::is_zero(r)) {
+    x.set_zero();
+    return x;
+  }
+  pack_limbs<PB>(x, r);
   x.exp = r.e;
   x.sign = r.s ? -1 : 1;
   return x;
 }
 }  // namespace detail
+
+/* ---------------- conversions through the core ---------------- */
+namespace detail {
+/* r = sign s, a left-justified 64-bit magnitude T (bit 63 set) times
+ * 2^(e - 64), rounded to the core's N words (only N = 1 loses bits) */
+template <int N>
+__host__ __device__ inline void from_top64(mpb::fval<N> &r, uint64_t T, int32_t e, uint32_t s) {
+  for (int i = 0; i < N; i++) r.m[i] = 0u;
+  r.m[N - 1] = (uint32_t)(T >> 32);
+  uint32_t rb = 0u, st = 0u;
+  if (N >= 2)
+    r.m[N - 2] = (uint32_t)T;
+  else {
+    rb = (uint32_t)(T >> 31) & 1u;
+    st = (uint32_t)T & 0x7fffffffu;
+  }
+  r.e = e;
+  r.s = s;
+  mpb::rndn<N>(r.m, r.e, rb, st);
+}
+/* the core value x rounded (RNDN) or widened (exactly) to NT words */
+template <int NT, int NF>
+__host__ __device__ inline void resize(mpb::fval<NT> &r, const mpb::fval<NF> &x) {
+  if (mpb::is_zero(x)) {
+    mpb::set_zero(r);
+    return;
+  }
+  /* word i of r is word i + NF - NT of x (0 below x) */
+  for (int i = 0; i < NT; i++) r.m[i] = (i + NF - NT >= 0) ? x.m[i + NF - NT] : 0u;
+  r.e = x.e;
+  r.s = x.s;
+  if (NT < NF) {
+    const uint32_t g = x.m[NF - NT - 1];
+    uint32_t st = g << 1;
+    for (int i = 0; i < NF - NT - 1; i++) st |= x.m[i];
+    mpb::rndn<NT>(r.m, r.e, g >> 31, st);
+  }
+}
+}  // namespace detail
+
+template <int PB>
+__host__ __device__ cu_freal<PB> cu_freal<PB>::finalize(const cu_limb *D, int len, int msb, long Ehi, cu_limb brnd,
+                                                        cu_limb bsti, int sgn) {
+  typedef typename detail::core_of<PB>::type V;
+  const int NW = detail::core_of<PB>::N32;
+  if (msb < 0) {
+    cu_freal r;
+    r.set_zero();
+    return r;
+  }
+  /* word NW-1-w of the result holds D's bits [msb - 32 w - 31, msb - 32 w] */
+  V v;
+  for (int w = 0; w < NW; w++) v.m[NW - 1 - w] = detail::dbits32(D, len, (long)msb - 32L * w - 31);
+  const long last = (long)msb - PB + 1; /* D position of the result's last bit */
+  uint32_t rb = 0u, st = 0u;
+  if (last > 0) { /* the round bit is a bit of D; D's lower bits and brnd/bsti are sticky */
+    rb = (uint32_t)cu_wbit(D, len, last - 1);
+    st = (uint32_t)(cu_wsticky_below(D, len, last - 1) | brnd | bsti);
+  } else if (last == 0) { /* the round bit is the bit just under D */
+    rb = (uint32_t)(brnd & 1ull);
+    st = (uint32_t)(bsti != 0ull);
+  } /* last < 0: every significant bit fits, the value is exact */
+  v.e = (int32_t)(Ehi + 1);
+  v.s = sgn < 0 ? 1u : 0u;
+  const int32_t e0 = v.e;
+  mpb::rndn<NW>(v.m, v.e, rb, st);
+  cu_freal r;
+  detail::pack_limbs<PB>(r, v);
+  r.exp = (long)Ehi + 1 + (long)(v.e - e0); /* the 64-bit exponent, plus the rounding's carry */
+  r.sign = sgn;
+  return r;
+}
+
+template <int PB>
+__host__ __device__ cu_freal<PB> cu_freal<PB>::from_double(double d) {
+  typename detail::core_of<PB>::type v;
+  if (d == 0.0) {
+    mpb::set_zero(v);
+    return detail::from_core<PB>(v);
+  }
+  int k;
+  const double f = frexp(fabs(d), &k);                     /* |d| = f 2^k, f in [1/2, 1) */
+  const uint64_t F = (uint64_t)ldexp(f, 64);               /* f's 53 bits, left-justified */
+  detail::from_top64(v, F, (int32_t)k, d < 0 ? 1u : 0u);
+  return detail::from_core<PB>(v);
+}
+
+template <int PB>
+__host__ __device__ double cu_freal<PB>::to_double() const {
+  if (is_zero()) return 0.0;
+  const int NW = detail::core_of<PB>::N32;
+  typename detail::core_of<PB>::type v;
+  detail::to_core<PB>(v, *this);
+  if (PB > 53) mpb::round_to_bits<NW>(v, 53); /* the nearest 53-bit value */
+  /* the value is (top two words) * 2^(e - 64); for PB = 32 only one word */
+  const uint64_t T = ((uint64_t)v.m[NW - 1] << 32) | (NW >= 2 ? v.m[NW - 2] : 0u);
+  const double mag = ldexp((double)T, v.e - 64); /* T has at most 53 significant bits: exact */
+  return sign < 0 ? -mag : mag;
+}
 
 /* N x N -> 2N (64-bit limbs) exact product (reference cu_freal.cuh:173-200) */
 template <int PB>
@@ -244,13 +302,16 @@ __host__ __device__ static cu_freal<PB> cu_fmul(const cu_freal<PB> &a, const cu_
   return detail::from_core<PB>(r);
 }
 
-/* magnitude compare (reference cu_cmpmag, cu_freal.cuh:215-222) */
+/* magnitude compare, -1 / 0 / 1 (reference cu_cmpmag, cu_freal.cuh:215-222):
+ * the exponents first, then the significands word by word from the top, by
+ * the core */
 template <int PB>
 __host__ __device__ static int cu_cmpmag(const cu_freal<PB> &a, const cu_freal<PB> &b) {
-  if (a.exp != b.exp) return a.exp > b.exp ? 1 : -1;
-  for (int i = cu_freal<PB>::N - 1; i >= 0; i--)
-    if (a.m[i] != b.m[i]) return a.m[i] > b.m[i] ? 1 : -1;
-  return 0;
+  typename detail::core_of<PB>::type x, y;
+  detail::to_core<PB>(x, a);
+  detail::to_core<PB>(y, b);
+  if (a.is_zero() || b.is_zero()) return (int)!a.is_zero() - (int)!b.is_zero(); /* zero is the smallest */
+  return mpb::cmpmag(x, y);
 }
 
 /* round(|a| + |b|) with sign sgn (reference cu_addmag, cu_freal.cuh:224-245) */
@@ -329,65 +390,63 @@ template <int PB>
 __host__ __device__ static inline int cu_sgn(const cu_freal<PB> &a) {
   return a.is_zero() ? 0 : a.sign;
 }
+/* signed compare, -1 / 0 / 1 (reference cu_cmp, cu_freal.cuh:304-314):
+ * values of different signs (zero counting as sign 0) order by their sign;
+ * equal signs by magnitude, reversed for negative values */
 template <int PB>
 __host__ __device__ static int cu_cmp(const cu_freal<PB> &a, const cu_freal<PB> &b) {
-  if (a.is_zero() && b.is_zero()) return 0;
-  if (a.is_zero()) return b.sign > 0 ? -1 : 1;
-  if (b.is_zero()) return a.sign > 0 ? 1 : -1;
-  if (a.sign != b.sign) return a.sign > 0 ? 1 : -1;
-  const int m = cu_cmpmag<PB>(a, b);
-  return a.sign > 0 ? m : -m;
+  const int sa = cu_sgn<PB>(a), sb = cu_sgn<PB>(b);
+  if (sa != sb) return sa < sb ? -1 : 1;
+  return sa * cu_cmpmag<PB>(a, b); /* 0 when both are zero */
 }
-/* re-round to another precision, exact when widening (reference cu_freal.cuh:316-323) */
+/* the value at another precision: widened exactly or rounded to nearest-even
+ * (reference cu_convert, cu_freal.cuh:316-323), through the core words */
 template <int TO, int FROM>
 __host__ __device__ static inline cu_freal<TO> cu_convert(const cu_freal<FROM> &x) {
-  if (x.is_zero()) {
-    cu_freal<TO> r;
-    r.set_zero();
-    return r;
-  }
-  return cu_freal<TO>::finalize(x.m, cu_freal<FROM>::N, cu_freal<FROM>::N * 64 - 1, x.exp - 1, 0, 0, x.sign);
+  typename detail::core_of<FROM>::type v;
+  typename detail::core_of<TO>::type r;
+  detail::to_core<FROM>(v, x);
+  detail::resize(r, v);
+  return detail::from_core<TO>(r);
 }
-/* exact small integer (reference cu_freal.cuh:325-334) */
+/* an integer, exact from PB = 64 up and rounded to nearest below (reference
+ * cu_from_si, cu_freal.cuh:325-334): the magnitude is left-justified by its
+ * leading-zero count and handed to the core */
 template <int PB>
 __host__ __device__ static cu_freal<PB> cu_from_si(long v) {
-  cu_freal<PB> r;
+  typename detail::core_of<PB>::type r;
   if (v == 0) {
-    r.set_zero();
-    return r;
+    mpb::set_zero(r);
+    return detail::from_core<PB>(r);
   }
-  const int sgn = v < 0 ? -1 : 1;
-  unsigned long long a = v < 0 ? (unsigned long long)(-(v + 1)) + 1ULL : (unsigned long long)v;
-  int nb = 64;
-  while (!((a >> (nb - 1)) & 1)) nb--;
-  return cu_freal<PB>::finalize(&a, 1, nb - 1, (long)nb - 1, 0, 0, sgn);
+  const uint64_t mag = v < 0 ? 0ull - (uint64_t)v : (uint64_t)v; /* |v|, LONG_MIN included */
+  int lz = 0;
+  while (!((mag << lz) >> 63)) lz++;
+  detail::from_top64(r, mag << lz, (int32_t)(64 - lz), v < 0 ? 1u : 0u);
+  return detail::from_core<PB>(r);
 }
-/* round to nearest integer, ties to even (reference cu_freal.cuh:336-356) */
+/* the nearest integer, ties to even (reference cu_lround, cu_freal.cuh:336-356;
+ * |x| must stay below 2^62 as there): with MPFR exponent e, |x| < 2^e, so
+ * rounding the significand to its top e bits (the core's round_to_bits) leaves
+ * the integer in those bits; e <= 0 means |x| < 1/2 (0) or, for e = 0,
+ * |x| in [1/2, 1), which is 1 except for the tie 1/2 (0, the even neighbour) */
 template <int PB>
 __host__ __device__ static long cu_lround(const cu_freal<PB> &x) {
-  if (x.is_zero()) return 0;
-  const int N = cu_freal<PB>::N;
-  const long e = x.exp;
-  if (e <= 0) {
-    if (e == 0) {
-      bool half = (x.m[N - 1] == (1ULL << 63));
-      for (int i = 0; i < N - 1; i++) half &= (x.m[i] == 0);
-      const long r = half ? 0 : 1;
-      return x.sign < 0 ? -r : r;
-    }
-    return 0;
+  if (x.is_zero() || x.exp < 0) return 0;
+  const int NW = detail::core_of<PB>::N32;
+  typename detail::core_of<PB>::type v;
+  detail::to_core<PB>(v, x);
+  long mag;
+  if (x.exp == 0) {
+    bool tie = v.m[NW - 1] == 0x80000000u;
+    for (int i = 0; i < NW - 1; i++) tie = tie && v.m[i] == 0u;
+    mag = tie ? 0 : 1;
+  } else {
+    if (x.exp < PB) mpb::round_to_bits<NW>(v, (int)x.exp); /* may carry: v.e = e + 1 */
+    const uint64_t T = ((uint64_t)v.m[NW - 1] << 32) | (NW >= 2 ? v.m[NW - 2] : 0u);
+    mag = v.e >= 64 ? (long)T : (long)(T >> (64 - v.e)); /* the top v.e bits */
   }
-  unsigned long long ip = 0;
-  for (long b = 0; b < e; b++) {
-    const long bit = (long)N * 64 - e + b;
-    ip |= ((x.m[bit >> 6] >> (bit & 63)) & 1ULL) << b;
-  }
-  const long rb = (long)N * 64 - e - 1;
-  const unsigned long long rbit = rb >= 0 ? ((x.m[rb >> 6] >> (rb & 63)) & 1ULL) : 0;
-  const unsigned long long st = cu_wsticky_below(x.m, N, rb);
-  if (rbit && (st || (ip & 1))) ip++;
-  const long r = (long)ip;
-  return x.sign < 0 ? -r : r;
+  return x.sign < 0 ? -mag : mag;
 }
 
 /* operators (reference cu_freal.cuh:358-364) */

@@ -56,6 +56,8 @@
  * mpb_gemm_exact_c_workspace): digit planes nprod*S*(m+n)*kp bytes and the
  * diagonal planes nprod*P*(2S-1)*m*n*4 bytes.
  */
+#include <atomic>
+
 #include "exact_gemm.cuh"
 
 namespace mpb {
@@ -438,19 +440,24 @@ constexpr size_t kStaticScratchBytes = (size_t)16 << 20;
 static __device__ __align__(256) uint8_t g_exact_scratch[kStaticScratchBytes];
 
 /* Device address of g_exact_scratch on the current device.  The host-side
- * name is only a stand-in, so the address is looked up once per device (the
- * first call on a device, which should therefore come before any stream
- * capture) with that device current. */
+ * name is only a stand-in, so the address is looked up with that device
+ * current, by the first call on the device that succeeds in doing so (that
+ * first call should come before any stream capture).  Only a successful
+ * lookup is kept: a lookup that fails (no context yet, a capture in progress)
+ * returns nullptr for that call, and the next call tries again. */
 uint8_t *static_scratch() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-  static std::once_flag once[64];
-  static uint8_t *addr[64];
-  std::call_once(once[dev], [dev] {
-    void *p = nullptr;
-    addr[dev] = (cudaGetSymbolAddress(&p, g_exact_scratch) == cudaSuccess) ? (uint8_t *)p : nullptr;
-  });
-  return addr[dev];
+  static std::atomic<uint8_t *> addr[64];
+  uint8_t *a = addr[dev].load(std::memory_order_acquire);
+  if (a) return a;
+  void *p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_exact_scratch) != cudaSuccess || !p) {
+    (void)cudaGetLastError(); /* do not leave the failure for the caller's next check */
+    return nullptr;
+  }
+  addr[dev].store((uint8_t *)p, std::memory_order_release); /* the same address whichever thread wins */
+  return (uint8_t *)p;
 }
 }  // namespace
 

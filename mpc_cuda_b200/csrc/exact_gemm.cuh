@@ -476,9 +476,15 @@ __device__ __forceinline__ bool round_words(fval<N> &r, uint32_t (&v)[W], long l
   if (cert >= 0) {
     const long t = cert - (msb - 32L * N + 1); /* log2 of the bound in ULPs */
     const uint64_t G = ((uint64_t)g << 32) | v[W - N - 2];
-    const uint64_t thr = (t < -64) ? 1ull : (1ull << (64 + t)); /* >= the bound, in 2^-64 ULPs */
+    /* the bound in 2^-64 ULPs (rounded up); only t <= -3 can certify, so the
+     * shift is taken only there, where 64 + t < 62 */
     const uint64_t half = 1ull << 63;
-    ok = t <= -3 && (G <= half - thr - 1 || G > half + thr);
+    if (t > -3) {
+      ok = false;
+    } else {
+      const uint64_t thr = (t < -64) ? 1ull : (1ull << (64 + t));
+      ok = G <= half - thr - 1 || G > half + thr;
+    }
   }
   int32_t ee = (int32_t)(msb + 1 + lsb_exp);
   rndn<N>(r.m, ee, g >> 31, st);
@@ -529,9 +535,13 @@ __device__ __forceinline__ bool round_regs(fval<N> &r, uint32_t (&v)[W], uint32_
   if (cert >= 0) {
     const long t = cert - (msb - 32L * N + 1); /* log2 of the bound in ULPs */
     const uint64_t G = ((uint64_t)g << 32) | nx;
-    const uint64_t thr = (t < -64) ? 1ull : (1ull << (64 + t));
     const uint64_t half = 1ull << 63;
-    ok = t <= -3 && (G <= half - thr - 1 || G > half + thr);
+    if (t > -3) {
+      ok = false;
+    } else {
+      const uint64_t thr = (t < -64) ? 1ull : (1ull << (64 + t));
+      ok = G <= half - thr - 1 || G > half + thr;
+    }
   }
   int32_t ee = (int32_t)(msb + 1 + lsb_exp);
   rndn<N>(r.m, ee, g >> 31, st);

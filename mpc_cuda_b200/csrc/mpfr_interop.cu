@@ -97,7 +97,14 @@ int to_mpfr_one(int prec, const uint8_t *e, mpfr_view *z) {
     return MPB_OK;
   }
   const int nd = (int)((z->prec + 63) / 64);
-  z->exp = (long)h->exp + round_limbs(z->d, nd, z->prec, m, n64);
+  std::vector<uint64_t> d((size_t)nd);
+  const long e2 = (long)h->exp + round_limbs(d.data(), nd, z->prec, m, n64);
+  /* MPFR's default exponent range is [1 - 2^30, 2^30 - 1]; a value outside it
+   * (possible after a carry at the top, or from a head at the range's edge)
+   * would make an invalid mpfr_t, so it is refused and z is left unchanged */
+  if (e2 > (1L << 30) - 1 || e2 < 1 - (1L << 30)) return MPB_ERR_ARG;
+  std::memcpy(z->d, d.data(), 8u * (size_t)nd);
+  z->exp = e2;
   z->sign = h->sign < 0 ? -1 : 1;
   return MPB_OK;
 }
@@ -108,16 +115,21 @@ int from_mpfr_one(int prec, const mpfr_view *z, uint8_t *e) {
   uint64_t *m = (uint64_t *)(e + 16);
   if (!z) return MPB_ERR_NULL;
   if (z->exp == kExpNanMpfr || z->exp == kExpInfMpfr) return MPB_ERR_ARG; /* no NaN or infinity here */
-  h->pad = 0;
   if (z->exp == kExpZeroMpfr) {
+    h->pad = 0;
     h->sign = 1;
     h->exp = kAosZeroExp;
     std::memset(m, 0, 8u * (size_t)n64);
     return MPB_OK;
   }
   const int ns = (int)((z->prec + 63) / 64);
-  const long e2 = z->exp + round_limbs(m, n64, prec, z->d, ns);
-  if (e2 >= (1L << 30) || e2 <= -(1L << 30)) return MPB_ERR_ARG; /* outside the engine's exponent range */
+  uint64_t d[32]; /* n64 <= 32 (PB <= 2048) */
+  const long e2 = z->exp + round_limbs(d, n64, prec, z->d, ns);
+  /* outside the engine's exponent range: refused before anything is written,
+   * so the element keeps its old value */
+  if (e2 >= (1L << 30) || e2 <= -(1L << 30)) return MPB_ERR_ARG;
+  std::memcpy(m, d, 8u * (size_t)n64);
+  h->pad = 0;
   h->exp = e2;
   h->sign = z->sign < 0 ? -1 : 1;
   return MPB_OK;

@@ -30,9 +30,18 @@ _LIB = None
 _REF = None
 
 
+# where the reference tree is mounted in the build container (read-only); the
+# GPU machines have no copy and use the libraries built here
+REFERENCE_TREE = os.environ.get("MPB_REFERENCE_TREE", "/root/reference")
+
+
 def build(quiet: bool = True) -> None:
-    """Compile liboracle.so (and _ref/libref_host.so when the reference tree exists)."""
-    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    """Compile liboracle.so, and _ref/libref_host.so when the reference tree exists."""
+    cmd = ["make", "-C", HERE]
+    inc = os.path.join(REFERENCE_TREE, "include")
+    if os.path.isfile(os.path.join(inc, "mpc_cuda", "cu_freal.cuh")):
+        cmd.append("REF_INCLUDE=" + inc)
+    out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:

@@ -267,6 +267,77 @@ void t_cfn(int fn, long n, const void *A, const void *B, void *R) {
   }
 }
 
+/* utilities over AoS arrays (test surface): op 0 cu_cmp(a, b), 1 cu_cmpmag(a, b),
+ * 2 cu_lround(a) into iv; 3 cu_from_si(iv) into r */
+template <int PB>
+void util1(int op, long n, const void *A, const void *B, long *iv, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto b = (const cu_freal<PB> *)B;
+  auto r = (cu_freal<PB> *)R;
+  for (long i = 0; i < n; i++) {
+    switch (op) {
+      case 0: iv[i] = cu_fp::cu_cmp<PB>(a[i], b[i]); break;
+      case 1: iv[i] = cu_fp::cu_cmpmag<PB>(a[i], b[i]); break;
+      case 2: iv[i] = cu_fp::cu_lround<PB>(a[i]); break;
+      default: r[i] = cu_fp::cu_from_si<PB>(iv[i]);
+    }
+  }
+}
+/* finalize over n rows: D row i = 4 limbs, q row i = { len, msb, Ehi, brnd, bsti, sgn } */
+template <int PB>
+void finalize1(long n, const unsigned long long *D, const long *q, void *R) {
+  auto r = (cu_freal<PB> *)R;
+  for (long i = 0; i < n; i++) {
+    const long *p = q + 6 * i;
+    r[i] = cu_freal<PB>::finalize(D + 4 * i, (int)p[0], (int)p[1], p[2], (unsigned long long)p[3],
+                                  (unsigned long long)p[4], (int)p[5]);
+  }
+}
+/* exact product terms (test surface): hdr row i = { sign, exp, zero } and the
+ * WN limbs of cu_mk_term(a[i], b[i]); r[i] = cu_round_sum2 of that term and
+ * the negated term of (c[i], d[i]) */
+template <int PB>
+void terms1(long n, const void *A, const void *B, const void *Cc, const void *Dd, long *hdr,
+            unsigned long long *M, void *R) {
+  auto a = (const cu_freal<PB> *)A;
+  auto b = (const cu_freal<PB> *)B;
+  auto c = (const cu_freal<PB> *)Cc;
+  auto d = (const cu_freal<PB> *)Dd;
+  auto r = (cu_freal<PB> *)R;
+  const int WN = cu_fp::cu_wterm<PB>::WN;
+  for (long i = 0; i < n; i++) {
+    const cu_fp::cu_wterm<PB> t = cu_fp::cu_mk_term<PB>(a[i], b[i]);
+    hdr[3 * i] = t.sign;
+    hdr[3 * i + 1] = t.exp;
+    hdr[3 * i + 2] = t.zero ? 1 : 0;
+    for (int k = 0; k < WN; k++) M[(long)WN * i + k] = t.M[k];
+    cu_fp::cu_wterm<PB> u = cu_fp::cu_mk_term<PB>(c[i], d[i]);
+    u.sign = -u.sign;
+    r[i] = cu_fp::cu_round_sum2<PB>(t, u);
+  }
+}
+template <int TO, int FROM>
+void convert1(long n, const void *X, void *R) {
+  auto x = (const cu_freal<FROM> *)X;
+  auto r = (cu_freal<TO> *)R;
+  for (long i = 0; i < n; i++) r[i] = cu_fp::cu_convert<TO, FROM>(x[i]);
+}
+#define UTIL_SMALL_DISPATCH(P, CALL)                          \
+  switch (P) {                                                \
+    case 32: { constexpr int PB = 32; CALL; } break;          \
+    case 96: { constexpr int PB = 96; CALL; } break;          \
+    case 160: { constexpr int PB = 160; CALL; } break;        \
+    case 256: { constexpr int PB = 256; CALL; } break;        \
+    case 288: { constexpr int PB = 288; CALL; } break;        \
+    case 1056: { constexpr int PB = 1056; CALL; } break;      \
+    default: return -1;                                       \
+  }
+template <int TO>
+int convert_to(int from, long n, const void *X, void *R) {
+  UTIL_SMALL_DISPATCH(from, (convert1<TO, PB>(n, X, R)))
+  return 0;
+}
+
 #define REF_DISPATCH(P, CALL)                                                                   \
   switch (P) {                                                                                  \
     case 32: { constexpr int PB = 32; CALL; } return 0;                                         \
@@ -325,4 +396,20 @@ int ref_gemm_c(int P, long m, long n, long k, const void *A, long lda, const voi
 }
 int ref_from_double(int P, long n, const double *d, void *R) { REF_DISPATCH(P, t_from_double<PB>(n, d, R)) }
 int ref_to_double(int P, long n, const void *X, double *d) { REF_DISPATCH(P, t_to_double<PB>(n, X, d)) }
+int ref_util(int op, int P, long n, const void *A, const void *B, long *iv, void *R) {
+  if (op < 0 || op > 3) return -2;
+  REF_DISPATCH(P, util1<PB>(op, n, A, B, iv, R))
+}
+int ref_finalize(int P, long n, const unsigned long long *D, const long *q, void *R) {
+  REF_DISPATCH(P, finalize1<PB>(n, D, q, R))
+}
+int ref_terms(int P, long n, const void *A, const void *B, const void *Cc, const void *Dd, long *hdr,
+                 unsigned long long *M, void *R) {
+  REF_DISPATCH(P, terms1<PB>(n, A, B, Cc, Dd, hdr, M, R))
+}
+/* cu_convert<to, from> for to, from in {32, 96, 160, 256, 288, 1056} */
+int ref_convert(int to, int from, long n, const void *X, void *R) {
+  UTIL_SMALL_DISPATCH(to, return convert_to<PB>(from, n, X, R))
+  return -1;
+}
 }

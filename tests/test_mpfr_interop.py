@@ -130,3 +130,46 @@ def test_mpc_round_trip(orc, mpb, mpfr, prec):
     assert lib.mpb_caos_from_mpc(prec, n, ptrs, _p(back)) == 0
     assert (back == A).all()
     _free(L, arr)
+
+
+def _elem(prec, sign, exp, limbs):
+    """One AoS cu_freal<prec> element: { int sign; long exp; uint64 m[] }."""
+    n64 = (prec + 63) // 64
+    e = np.zeros(16 + 8 * n64, np.uint8)
+    e[0:4] = np.array([sign], np.int32).view(np.uint8)
+    e[8:16] = np.array([exp], np.int64).view(np.uint8)
+    e[16:] = np.array(limbs, np.uint64).view(np.uint8)
+    return e.reshape(1, -1)
+
+
+def test_mpfr_exponent_range_edges(mpb, mpfr):
+    """Results outside MPFR's default exponent range [1 - 2^30, 2^30 - 1] are
+    refused (MPB_ERR_ARG) in both directions, and the destination keeps its
+    old value; values at the edges themselves convert."""
+    L, lib, prec = mpfr, mpb.lib(), 128
+    emax, emin = (1 << 30) - 1, 1 - (1 << 30)
+    ones = [0xFFFFFFFFFFFFFFFF, 0xFFFFFFFFFFFFFFFF]
+    top = [0, 1 << 63]
+    z, pz = _objs(L, 64, 1)
+    L.mpfr_set_zero(C.byref(z[0]), 1)
+    # at the top edge without a carry: converts
+    assert lib.mpb_aos_to_mpfr(prec, 1, _p(_elem(prec, 1, emax, top)), pz) == 0
+    assert z[0].exp == emax
+    # 1 - 2^-128 at 2^emax rounds to 2^(emax+1) at 64 bits: refused, unchanged
+    assert lib.mpb_aos_to_mpfr(prec, 1, _p(_elem(prec, 1, emax, ones)), pz) == -7
+    assert z[0].exp == emax
+    # the bottom edge converts, one below it (a head the engine can hold) is refused
+    assert lib.mpb_aos_to_mpfr(prec, 1, _p(_elem(prec, -1, emin, top)), pz) == 0
+    assert z[0].exp == emin and z[0].sign == -1
+    assert lib.mpb_aos_to_mpfr(prec, 1, _p(_elem(prec, 1, emin - 1, top)), pz) == -7
+    assert z[0].exp == emin and z[0].sign == -1
+    _free(L, z)
+    # from a 128-bit mpfr_t of all ones at 2^emax into 64 bits: the carry leaves
+    # the engine's range, so the element is refused and keeps its old limbs and head
+    w, pw = _objs(L, prec, 1)
+    assert lib.mpb_aos_to_mpfr(prec, 1, _p(_elem(prec, 1, emax, ones)), pw) == 0
+    old = _elem(64, 1, 5, [0x8000000000000001])
+    out = old.copy()
+    assert lib.mpb_aos_from_mpfr(64, 1, pw, _p(out)) == -7
+    assert (out == old).all()
+    _free(L, w)
