@@ -1054,6 +1054,125 @@ def run_gpu(args):
     return 0
 
 
+# ------------------------------------------------------------------ drop-in user kernels
+DROPIN_PRECS = (64, 96, 128, 160, 256, 288, 512, 1024, 1056, 2048)
+
+
+def _uk_lib(path, pre):
+    import ctypes as C
+
+    L = C.CDLL(path)
+    I, Lg, V, D = C.c_int, C.c_long, C.c_void_p, C.c_double
+    for f in ("axpy_r", "axpy_c"):
+        getattr(L, pre + f).argtypes = [I, Lg, V, V, V, V, I, I, V]
+    getattr(L, pre + "axpy_d").argtypes = [I, Lg, D, V, V, V, I, I, V]
+    getattr(L, pre + "caxpy_d").argtypes = [I, Lg, D, D] + [V] * 6 + [I, I, V]
+    return L
+
+
+def run_dropin(args):
+    """Kernels written against the cu_fp surface (tests/dropin/user_kernels.cu)
+    compiled through this repository's drop-in headers and, beside them, the
+    same source compiled against the reference's own headers
+    (oracle/_ref/libref_user_kernels.so), timed on the same GPU and data:
+    AXPY over device AoS arrays of full-precision cu_freal / cu_fcomplex
+    (n = 2^20 real, 2^18 complex; rotating sets larger than L2) and the
+    reference's benchmark kernel (demos/bench_3way.cu:44-59: FP64 in and out,
+    N = 4096, <<<128, 32>>>, the configuration of its published table)."""
+    import torch
+
+    import oracle as O
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    uk = _uk_lib(os.path.join(ROOT, "tests", "dropin", "libuser_kernels.so"), "uk_")
+    ref_path = os.path.join(ROOT, "oracle", "_ref", "libref_user_kernels.so")
+    refuk = _uk_lib(ref_path, "refuk_") if os.path.exists(ref_path) else None
+
+    def timed(fn, reps):
+        for _ in range(args.warmup):
+            fn(0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(reps):
+            fn(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    clocks = Clocks(0)
+    clocks.start()
+    rows = []
+    for prec in DROPIN_PRECS:
+        es = O.elem_bytes(prec)
+        row = {"prec": prec}
+        for kind, n in (("real", 1 << 20), ("complex", 1 << 18)):
+            cplx = kind == "complex"
+            if prec >= 1024:
+                n >>= 2
+            X, Y = O.gen_pairs(prec, n, 0xD00D + prec, cplx=cplx)
+            a = O.gen_pairs(prec, 1, 0xD00E + prec, cplx=cplx)[0]
+            eb = es * (2 if cplx else 1)
+            nsets = max(2, -(-2 * L2_BYTES // (3 * n * eb)))
+            ta = torch.from_numpy(a.reshape(-1).copy()).to(dev)
+            sets = []
+            for _ in range(nsets):
+                sets.append((torch.from_numpy(X.reshape(-1).copy()).to(dev),
+                             torch.from_numpy(Y.reshape(-1).copy()).to(dev),
+                             torch.empty(n * eb, dtype=torch.uint8, device=dev)))
+            fname = "axpy_c" if cplx else "axpy_r"
+            entry = {}
+            for tag, L, pre in (("dropin", uk, "uk_"), ("reference", refuk, "refuk_")):
+                if L is None:
+                    continue
+                f = getattr(L, pre + fname)
+
+                def go(i, f=f):
+                    x, y, z = sets[i % nsets]
+                    rc = f(prec, n, ta.data_ptr(), x.data_ptr(), y.data_ptr(), z.data_ptr(), 0, 128, sp)
+                    assert rc == 0, rc
+
+                reps = max(5, min(2000, int(2e9 / (n * (4 if cplx else 1) * (prec // 32) ** 2 * 30))))
+                t = timed(go, reps)
+                entry[tag] = {"mp_fma_per_s": round(n / t, 1), "ms": round(t * 1e3, 4)}
+            if "reference" in entry:
+                entry["dropin_over_reference"] = round(entry["reference"]["ms"] / entry["dropin"]["ms"], 3)
+            entry["n"] = n
+            row[kind] = entry
+            del sets
+        # the reference's benchmark kernel: FP64 in/out, N = 4096, <<<128, 32>>>
+        rng = np.random.default_rng(prec)
+        N = 4096
+        x, y = (torch.from_numpy(rng.uniform(-1, 1, N)).to(dev) for _ in range(2))
+        o = torch.empty(N, dtype=torch.float64, device=dev)
+        b3 = {}
+        for tag, L, pre in (("dropin", uk, "uk_"), ("reference", refuk, "refuk_")):
+            if L is None:
+                continue
+            f = getattr(L, pre + "axpy_d")
+            t = timed(lambda i, f=f: f(prec, N, 1.5, x.data_ptr(), y.data_ptr(), o.data_ptr(), 128, 32, sp), 8)
+            b3[tag] = {"ms": round(t * 1e3, 4), "mp_fma_per_s": round(N / t, 1)}
+        row["bench_3way_fp64_io_n4096"] = b3
+        rows.append(row)
+        print(json.dumps(row), file=sys.stderr)
+    clk = clocks.stop()
+    head = next(r for r in rows if r["prec"] == 256)["real"]
+    line = {"metric": "drop-in user-kernel AXPY mp-FMA/s (cu_fp operators in a user kernel), "
+                      "reference header on the same GPU beside it",
+            "value": head["dropin"]["mp_fma_per_s"], "unit": "mp-FMA/s", "n_gpus": 1,
+            "steps": None, "warmup": args.warmup, "higher_is_better": True, "scaling": None,
+            "vs_baseline": None, "dtype": "u32 limbs (drop-in: 64-bit limbs in memory)", "data": "synthetic",
+            "config": {"workload": "user kernels through include/mpc_cuda headers: real AXPY PB=256 n=2^20 "
+                                   "(value), every PB and the complex / FP64-I/O forms in per_prec",
+                       "l2": "rotating input sets larger than L2"},
+            "clocks": clk, "per_prec": rows}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -1061,7 +1180,7 @@ def main():
                     help="timed steps (default: the workload's, about 2 s of GPU time)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("mpb", "reference"), default="mpb")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["dropin_axpy"], default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--problems", type=int, default=None,
@@ -1073,6 +1192,8 @@ def main():
         WORKLOADS["gemv_batch"] = lambda: GemvBatchWorkload("gemv_batch", args.problems, 0x5EED4)
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "dropin_axpy":
+        return run_dropin(args)
     if args.steps is None:
         args.steps = WORKLOADS[args.workload]().default_steps
     if args.impl == "reference":

@@ -271,37 +271,99 @@ MPB_HD void mul_ui_exact(uint32_t *o, const uint32_t *a, uint32_t k) {
  * translation unit, called from the series loops (code size and compile
  * time stay linear in the number of functions)
  * ------------------------------------------------------------------ */
+/* Up to kByValueLimbs limbs each operation is one out-of-line function taking
+ * and returning values (passed in registers); wider operands go by reference
+ * (passing them by value would spill). */
 template <int N>
-MPB_NOINLINE void w_mul(fval<N> &r, const fval<N> &a, const fval<N> &b) {
-  mul<N>(r, a, b);
+MPB_NOINLINE fval<N> w_op2_v(int op, fval<N> a, fval<N> b) {
+  fval<N> r;
+  switch (op) {
+    case 0: mul<N>(r, a, b); break;
+    case 1: add<N>(r, a, b); break;
+    case 2: sub<N>(r, a, b); break;
+    case 3: div<N>(r, a, b); break;
+    default: sqrt_<N>(r, a);
+  }
+  return r;
 }
 template <int N>
-MPB_NOINLINE void w_add(fval<N> &r, const fval<N> &a, const fval<N> &b) {
-  add<N>(r, a, b);
+MPB_NOINLINE void w_op2_r(int op, fval<N> &r, const fval<N> &a, const fval<N> &b) {
+  switch (op) {
+    case 0: mul<N>(r, a, b); break;
+    case 1: add<N>(r, a, b); break;
+    case 2: sub<N>(r, a, b); break;
+    case 3: div<N>(r, a, b); break;
+    default: sqrt_<N>(r, a);
+  }
 }
 template <int N>
-MPB_NOINLINE void w_sub(fval<N> &r, const fval<N> &a, const fval<N> &b) {
-  sub<N>(r, a, b);
+MPB_HD void w_op2(int op, fval<N> &r, const fval<N> &a, const fval<N> &b) {
+  if constexpr (N <= kByValueLimbs)
+    r = w_op2_v<N>(op, a, b);
+  else
+    w_op2_r<N>(op, r, a, b);
 }
 template <int N>
-MPB_NOINLINE void w_div(fval<N> &r, const fval<N> &a, const fval<N> &b) {
-  div<N>(r, a, b);
+MPB_HD void w_mul(fval<N> &r, const fval<N> &a, const fval<N> &b) {
+  w_op2<N>(0, r, a, b);
 }
 template <int N>
-MPB_NOINLINE void w_sqrt(fval<N> &r, const fval<N> &a) {
-  sqrt_<N>(r, a);
+MPB_HD void w_add(fval<N> &r, const fval<N> &a, const fval<N> &b) {
+  w_op2<N>(1, r, a, b);
 }
 template <int N>
-MPB_NOINLINE void w_div_ui(fval<N> &r, const fval<N> &a, uint32_t d) {
+MPB_HD void w_sub(fval<N> &r, const fval<N> &a, const fval<N> &b) {
+  w_op2<N>(2, r, a, b);
+}
+template <int N>
+MPB_HD void w_div(fval<N> &r, const fval<N> &a, const fval<N> &b) {
+  w_op2<N>(3, r, a, b);
+}
+template <int N>
+MPB_HD void w_sqrt(fval<N> &r, const fval<N> &a) {
+  w_op2<N>(4, r, a, a);
+}
+template <int N>
+MPB_NOINLINE fval<N> w_div_ui_v(fval<N> a, uint32_t d) {
+  fval<N> r;
+  div_ui<N>(r, a, d);
+  return r;
+}
+template <int N>
+MPB_NOINLINE void w_div_ui_r(fval<N> &r, const fval<N> &a, uint32_t d) {
   div_ui<N>(r, a, d);
 }
 template <int N>
-MPB_NOINLINE void w_fmma(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c, const fval<N> &d) {
-  fmma<N>(r, a, b, c, d);
+MPB_HD void w_div_ui(fval<N> &r, const fval<N> &a, uint32_t d) {
+  if constexpr (N <= kByValueLimbs)
+    r = w_div_ui_v<N>(a, d);
+  else
+    w_div_ui_r<N>(r, a, d);
 }
 template <int N>
-MPB_NOINLINE void w_fmms(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c, const fval<N> &d) {
-  fmms<N>(r, a, b, c, d);
+MPB_NOINLINE fval<N> w_fmmx_v(fval<N> a, fval<N> b, fval<N> c, fval<N> d, uint32_t negate_cd) {
+  fval<N> r;
+  fmms<N>(r, a, b, c, d, negate_cd);
+  return r;
+}
+template <int N>
+MPB_NOINLINE void w_fmmx_r(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c, const fval<N> &d,
+                           uint32_t negate_cd) {
+  fmms<N>(r, a, b, c, d, negate_cd);
+}
+template <int N>
+MPB_HD void w_fmma(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c, const fval<N> &d) {
+  if constexpr (N <= kByValueLimbs)
+    r = w_fmmx_v<N>(a, b, c, d, 0u);
+  else
+    w_fmmx_r<N>(r, a, b, c, d, 0u);
+}
+template <int N>
+MPB_HD void w_fmms(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c, const fval<N> &d) {
+  if constexpr (N <= kByValueLimbs)
+    r = w_fmmx_v<N>(a, b, c, d, 1u);
+  else
+    w_fmmx_r<N>(r, a, b, c, d, 1u);
 }
 
 /* ------------------------------------------------------------------ *

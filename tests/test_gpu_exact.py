@@ -288,3 +288,22 @@ def test_exact_complex_pb256_full_size(orc, mpb):
             g = got[sel][:, part * es:(part + 1) * es]
             w = e4[sel][:, part * e4s:(part + 1) * e4s]
             assert orc.ulp_errors(prec, g, 4 * prec, w).max() <= 0.5
+
+
+def test_plain_complex_pb256_full_size(orc, mpb):
+    """The plain per-operation-rounded complex GEMM on the same 512^3 PB=256
+    workload (the kernel the bench times beside the exact one): a row sample
+    (first, middle, last rows) must equal MPC's mpc_mul + mpc_add in k order."""
+    prec, m, n, k = 256, 512, 512, 512
+    (ar, ai), (br, bi) = synth.gemm_c256()
+    A, B = synth.interleave_complex(prec, ar, ai), synth.interleave_complex(prec, br, bi)
+    dA = to_dev(layout.aos_to_vec(prec, A, True))
+    dB = to_dev(layout.aos_to_vec(prec, B, True))
+    Cd = mpb.empty(prec, m * n, True)
+    mpb.gemm(prec, m, n, k, dA, k, dB, n, Cd, n, cplx=True)
+    got = layout.vec_to_aos(prec, to_host(Cd), m * n, True)
+    for r0, r1 in ((0, 2), (257, 258), (m - 1, m)):
+        sel = slice(r0 * n, r1 * n)
+        exp = orc.gemm(prec, m, n, k, A, k, B, n, cplx=True, impl="mp", rows=(r0, r1))
+        bad, first = orc.mismatches(prec, got[sel], exp[sel], True)
+        assert bad == 0, f"rows {r0}-{r1}: {bad} entries differ from MPC (first {first})"
