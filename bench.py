@@ -405,7 +405,38 @@ class GemmWorkload:
         torch.cuda.synchronize()
         plain_ms = e0.elapsed_time(e1) / steps
         st = self.status.cpu().tolist()
-        return {"plain_ms_per_step": plain_ms, "plain_value": self.units() / (plain_ms / 1e3), "status": st}
+        return {"plain_ms_per_step": plain_ms, "plain_value": self.units() / (plain_ms / 1e3), "status": st,
+                "accuracy": self.accuracy()}
+
+    def accuracy(self, rows=(0, None, -1)):
+        """Error of the timed exact GEMM's result on a row sample (first, middle
+        and last rows of C, every column): ULPs of PB bits against the dot
+        product rounded at 4 PB bits (MPFR mpfr_dot / MPC mpc_dot), and whether
+        every entry equals the correctly rounded dot product at PB bits."""
+        import oracle as O
+        from mpc_cuda_b200 import layout
+
+        A, B = self.host
+        c, p = self.cplx, self.prec
+        got = layout.vec_to_aos(p, self.dC.cpu().numpy(), self.m * self.n, c)
+        es, e4s = layout.aos_bytes(p), layout.aos_bytes(4 * p)
+        ulps, equal, picked = [], True, []
+        for r in rows:
+            r = self.m // 2 if r is None else (r % self.m)
+            picked.append(r)
+            sel = slice(r * self.n, (r + 1) * self.n)
+            want = O.gemm_exact(p, self.m, self.n, self.k, A, self.k, B, self.n, cplx=c, impl="mp", rows=(r, r + 1))
+            equal = equal and O.mismatches(p, got[sel], want[sel], c)[0] == 0
+            w4 = O.gemm_exact(p, self.m, self.n, self.k, A, self.k, B, self.n, cplx=c, out_prec=4 * p,
+                              rows=(r, r + 1))
+            for part in ((0, 1) if c else (0,)):
+                ulps.append(O.ulp_errors(p, got[sel][:, part * es:(part + 1) * es], 4 * p,
+                                         w4[sel][:, part * e4s:(part + 1) * e4s]))
+        u = np.concatenate(ulps)
+        return {"rows": picked, "entries": int(u.size), "ulp_max": float(u.max()), "ulp_mean": float(u.mean()),
+                "reference": f"{'mpc_dot' if c else 'mpfr_dot'} at {4 * p} bits"
+                             + (", per component" if c else ""),
+                "equal_to_correctly_rounded_dot": bool(equal)}
 
     def roofline_tensor(self, tensor_ms, int8_ops):
         ops = 2.0 * self.nprod * self.units() * self.pairs
@@ -564,7 +595,8 @@ class GemvBatchWorkload:
                         "peak_source": hbm_src},
                 "per_prec": {str(p): {"mp_fma": v[0], "imad_ops": v[1], "bytes": v[2],
                                       "solo_ms": round(tuned.get(p, -1.0), 4),
-                                      "tuning": list(self.batch.tuning()[p])} for p, v in sorted(w.items())}}
+                                      "tuning": list(self.batch.tuning()[p]),
+                                      "lanes_per_row": self.batch.splits()[p]} for p, v in sorted(w.items())}}
 
     def cpu_run(self, impl, count):
         """Problems in planned order until about count units; returns units done."""
@@ -802,6 +834,15 @@ class CfnWorkload(AxpyWorkload):
                 "l2": f"{self.nsets} rotating input sets > L2"}
 
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# the dominant kernel, from one ncu capture of that kernel on this workload
+# (the summaries under profiles/ give the commands); None where no capture exists
+NCU_TRAFFIC = {
+    "axpy_r256": (82.6e6, "k_axpy_r<8>, profiles/k_axpy_r_pb256_n1048576.md"),
+    "axpy_c1024": (180.0e6, "k_axpy_c<32>, profiles/k_axpy_c_pb1024_n262144.md"),
+    "gemm_r512": (1.388e9, "k_diag_gemm main pass, profiles/k_diag_gemm_gemm_r512_1024cube.md"),
+}
+
 WORKLOADS = {
     "cexp_c512": lambda: CfnWorkload("cexp_c512", "exp", 512, 1 << 18, 0x5EEDB),
     "div_r512": lambda: DivSqrtWorkload("div_r512", "div", 512, 1 << 20, 0x5EED6),
@@ -931,6 +972,17 @@ class E2EPipeline:
                 self.main.wait_event(self.ev_out[s])
 
 
+def split_targets(wl):
+    """(kind, prec) of the thread-vs-warp split a workload's kernels read."""
+    import mpc_cuda_b200 as M
+
+    if isinstance(wl, AxpyWorkload) and wl.cplx:
+        return [(M.SPLIT_AXPY_C, wl.prec)]
+    if isinstance(wl, GemvBatchWorkload):
+        return [(M.SPLIT_GEMV_R, 1024), (M.SPLIT_GEMV_R, 2048)]
+    raise SystemExit(f"--split: workload {wl.name} has no warp-cooperative form")
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -958,6 +1010,11 @@ def run_gpu(args):
 
     wl = WORKLOADS[args.workload]()
     wl.with_e2e = not args.no_e2e
+    if args.split:
+        import mpc_cuda_b200 as M
+
+        for kind, prec in split_targets(wl):
+            M.set_split(kind, prec, args.split)
     wl.setup(rank, device)
     stream = torch.cuda.current_stream(device)
     sp = stream.cuda_stream
@@ -1022,6 +1079,8 @@ def run_gpu(args):
             roof = wl.roofline_tensor(tensor_ms, int8_peak_ops(device))
         else:
             roof = wl.roofline(kernel_s, peaks, imad_peak(sp))
+        if roof.get("traffic") is None and wl.name in NCU_TRAFFIC:
+            roof["traffic"], roof["traffic_source"] = NCU_TRAFFIC[wl.name]
         cpu = cpu_baseline(wl) if world == 1 and not args.no_cpu else None
         h2d, d2h = wl.e2e_bytes()
         line = {
@@ -1047,6 +1106,8 @@ def run_gpu(args):
                              "kernel": "k_gemm_r (sequential-k, per-operation rounding)"}
             line["exact_over_plain"] = line["value"] / extra["plain_value"]
             line["status"] = {"fallback_rows_cols": extra["status"][0], "kernel_error": extra["status"][1]}
+            if extra.get("accuracy"):
+                line["accuracy"] = extra["accuracy"]
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -1183,6 +1244,9 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["dropin_axpy"], default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--split", type=int, default=0,
+                    help="lanes per element for the kernels with a warp-cooperative form (mpb_set_split); "
+                         "0 keeps the library's default")
     ap.add_argument("--problems", type=int, default=None,
                     help="gemv_batch only: number of problems (profiling runs on a small case)")
     args = ap.parse_args()

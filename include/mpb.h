@@ -209,6 +209,20 @@ int mpb_gemm_r(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda
 int mpb_gemm_c(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
                void *C, size_t ldc, void *stream);
 
+/* ---- thread-vs-warp split ---- */
+/* Kernels with a warp-cooperative form for wide operands: one element (a
+ * complex AXPY element, a GEMV row) per thread, or per group of `lanes`
+ * lanes that hold its limbs between them (lanes 4 or 8 at 1024 bits, 8 or 16
+ * at 2048 bits; the complex AXPY has the cooperative form at 1024 bits).
+ * Results are identical either way; the split only changes the speed.  The
+ * setting is process-wide, read at every launch; the defaults are the
+ * fastest forms measured on B200.  No counterpart in the reference (its
+ * kernels are one thread per element, demos/bench_3way.cu:44-59).
+ * Returns MPB_ERR_ARG for a kind or lane count not offered at that precision. */
+enum { MPB_SPLIT_AXPY_C = 0, MPB_SPLIT_GEMV_R = 1 };
+int mpb_set_split(int kind, int prec, int lanes);
+int mpb_get_split(int kind, int prec, int *lanes);
+
 /* ---- batched GEMV: thousands of independent problems, mixed sizes and precisions ---- */
 /* One problem y_out = A.x + y (real, prec bits, same order as mpb_gemv_r).
  * Device pointers; lda a multiple of 32 (>= n); m or n may be 0. */
@@ -240,6 +254,11 @@ int mpb_batch_gemv_autotune(mpb_batch_plan *plan, void *stream);
  * multiple of 32 up to 256; persistent blocks per SM, 0 = occupancy limit). */
 int mpb_batch_gemv_get_tuning(const mpb_batch_plan *plan, int prec, int *block, int *blocks_per_sm);
 int mpb_batch_gemv_set_tuning(mpb_batch_plan *plan, int prec, int block, int blocks_per_sm);
+/* Read / install the thread-vs-warp split of a precision group: lanes per row
+ * (1, or 4 / 8 at 1024 bits, 8 / 16 at 2048 bits; see mpb_set_split).  The
+ * autotuner tries every split with every launch shape. */
+int mpb_batch_gemv_get_split(const mpb_batch_plan *plan, int prec, int *lanes);
+int mpb_batch_gemv_set_split(mpb_batch_plan *plan, int prec, int lanes);
 /* Time of one run of the precision's problems alone on the whole GPU, as
  * measured by the last mpb_batch_gemv_autotune (-1 before any; 0 when the
  * batch has no problem of that precision). */

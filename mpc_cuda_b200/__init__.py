@@ -88,6 +88,10 @@ _SIGS = {
     "mpb_batch_gemv_get_tuning": ([_V, _I, C.POINTER(_I), C.POINTER(_I)], C.c_int),
     "mpb_batch_gemv_set_tuning": ([_V, _I, _I, _I], C.c_int),
     "mpb_batch_gemv_tuned_ms": ([_V, _I, C.POINTER(C.c_float)], C.c_int),
+    "mpb_batch_gemv_get_split": ([_V, _I, C.POINTER(_I)], C.c_int),
+    "mpb_batch_gemv_set_split": ([_V, _I, _I], C.c_int),
+    "mpb_set_split": ([_I, _I, _I], C.c_int),
+    "mpb_get_split": ([_I, _I, C.POINTER(_I)], C.c_int),
     "mpb_batch_gemv_destroy": ([_V], None),
     "mpb_gemm_exact_workspace": ([_I, _S, _S, _S, _I], C.c_size_t),
     "mpb_profile_enable": ([_I], None),
@@ -341,6 +345,21 @@ def gemm_exact(prec, m, n, k, A, lda, B, ldb, Cm, ldc, sp_bits=32, workspace=Non
     return workspace
 
 
+# thread-vs-warp split of the kernels with a warp-cooperative form (mpb.h)
+SPLIT_AXPY_C, SPLIT_GEMV_R = 0, 1
+
+
+def set_split(kind, prec, lanes):
+    """Lanes per element for `kind` at `prec` (1 = one thread per element)."""
+    _call("mpb_set_split", int(kind), int(prec), int(lanes))
+
+
+def get_split(kind, prec):
+    v = C.c_int()
+    _call("mpb_get_split", int(kind), int(prec), C.byref(v))
+    return v.value
+
+
 class GemvProblem(C.Structure):
     """mpb_gemv_problem: y_out = A.x + y at precision prec (device pointers)."""
     _fields_ = [("prec", C.c_int), ("m", C.c_int), ("n", C.c_int), ("lda", C.c_size_t), ("A", C.c_void_p),
@@ -395,6 +414,18 @@ class BatchGemv:
     def set_tuning(self, table):
         for p, (b, s) in table.items():
             _call("mpb_batch_gemv_set_tuning", self._plan, int(p), int(b), int(s))
+
+    def splits(self):
+        """{prec: lanes per row} (1 = one thread per row, else a warp-cooperative group)."""
+        out = {}
+        for p in SUPPORTED:
+            v = C.c_int()
+            _call("mpb_batch_gemv_get_split", self._plan, p, C.byref(v))
+            out[p] = v.value
+        return out
+
+    def set_split(self, prec, lanes):
+        _call("mpb_batch_gemv_set_split", self._plan, int(prec), int(lanes))
 
     def close(self):
         if getattr(self, "_plan", None):

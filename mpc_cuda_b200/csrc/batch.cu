@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "coop_rows.cuh"
 
 namespace mpb {
 namespace batch {
@@ -55,10 +56,13 @@ struct DevProb { /* device copy of one problem */
 struct Tuning {
   int block;        /* threads per block (multiple of 32) */
   int blocks_per_sm; /* persistent grid: SMs x this (capped by occupancy) */
+  int lanes;        /* lanes per row: 1, or a warp-cooperative group (coop_rows.cuh) */
 };
 
-/* candidates tried by the autotuner */
-static const Tuning kCandidates[] = {{64, 2}, {64, 4}, {128, 1}, {128, 2}, {128, 4}, {256, 1}, {256, 2}};
+/* launch shapes tried by the autotuner, each with every split the precision offers */
+static const Tuning kCandidates[] = {{64, 2, 1}, {64, 4, 1}, {128, 1, 1}, {128, 2, 1},
+                                     {128, 4, 1}, {256, 1, 1}, {256, 2, 1}};
+static const Tuning kCoopCandidates[] = {{64, 0, 1}, {128, 0, 1}, {128, 4, 1}, {256, 0, 1}, {256, 2, 1}};
 
 template <int N>
 __global__ void __launch_bounds__(256) k_batch_gemv(const DevProb *probs, const int *order, const long long *prefix,
@@ -98,7 +102,64 @@ __global__ void __launch_bounds__(256) k_batch_gemv(const DevProb *probs, const 
   }
 }
 
+/* the same with G lanes per row: a warp takes a 32-row unit and runs it as G
+ * passes of 32/G rows (passes past the problem's last row are skipped) */
+template <int L, int G>
+__global__ void __launch_bounds__(256) k_batch_gemv_coop(const DevProb *probs, const int *order,
+                                                         const long long *prefix, int nprob, long long nunits,
+                                                         unsigned long long *counter) {
+  constexpr int N = G * L, RPW = 32 / G, SMW = coop_row_smem<N>::words;
+  extern __shared__ uint32_t sm_dyn[];
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = threadIdx.x >> 5, gw = (uint32_t)lane / G;
+  uint32_t *sm = sm_dyn + (warp * RPW + gw) * SMW;
+  while (true) {
+    long long u = 0;
+    if (lane == 0) u = (long long)atomicAdd(counter, 1ull);
+    u = __shfl_sync(0xffffffffu, u, 0);
+    if (u >= nunits) break;
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prefix[mid] <= u)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const DevProb pr = probs[order[lo]];
+    const long long blk = u - prefix[lo];
+    for (int pass = 0; pass < G; ++pass) {
+      const int r0 = (int)(blk * 32) + pass * RPW;
+      if (r0 >= pr.m) break; /* warp-uniform */
+      const int i = r0 + (int)gw;
+      const int ir = i < pr.m ? i : pr.m - 1;
+      coop::cv<L> acc;
+      coop_gemv_row<L, G>(acc, pr.A, (size_t)ir * pr.lda, (size_t)pr.n, pr.x, pr.y, (size_t)ir, sm);
+      if (i < pr.m) coop::store<L, G>(pr.yo, (size_t)i, acc);
+    }
+  }
+}
+template <int N>
+constexpr size_t coop_smem_bytes(int block, int G) {
+  return (size_t)(block / 32) * (size_t)(32 / G) * (size_t)coop_row_smem<N>::words * 4u;
+}
+
 using KernelFn = void (*)(const DevProb *, const int *, const long long *, int, long long, unsigned long long *);
+/* the kernel of group g at `lanes` lanes per row, and its dynamic shared memory per block */
+static KernelFn coop_kernel_of(int g, int lanes, int block, size_t *smem) {
+  if (g == 4) {
+    *smem = coop_smem_bytes<32>(block, lanes);
+    return lanes == 4 ? k_batch_gemv_coop<8, 4> : k_batch_gemv_coop<4, 8>;
+  }
+  *smem = coop_smem_bytes<64>(block, lanes);
+  return lanes == 8 ? k_batch_gemv_coop<8, 8> : k_batch_gemv_coop<4, 16>;
+}
+static bool lanes_ok(int g, int lanes) {
+  if (lanes == 1) return true;
+  if (g == 4) return lanes == 4 || lanes == 8;
+  if (g == 5) return lanes == 8 || lanes == 16;
+  return false;
+}
 static KernelFn kernel_of(int g) {
   switch (g) {
     case 0: return k_batch_gemv<2>;
@@ -205,9 +266,10 @@ extern "C" int mpb_batch_gemv_plan(int count, const mpb_gemv_problem *problems, 
     pl->gstart[g] = 0;
     pl->gcount[g] = 0;
     pl->gunits[g] = 0;
-    pl->tune[g] = Tuning{128, 0}; /* 0: full occupancy */
+    pl->tune[g] = Tuning{128, 0, 1}; /* 0: full occupancy */
     pl->tuned_ms[g] = -1.0f;
   }
+  for (int g = 4; g < kGroups; ++g) pl->tune[g].lanes = split_lanes(MPB_SPLIT_GEMV_R, 64 << g);
   for (int i = 0; i < count; ++i) {
     const mpb_gemv_problem &p = problems[i];
     hp[i] = DevProb{(const uint8_t *)p.A, (const uint8_t *)p.x, (const uint8_t *)p.y, (uint8_t *)p.y_out,
@@ -241,18 +303,20 @@ extern "C" int mpb_batch_gemv_plan(int count, const mpb_gemv_problem *problems, 
 
 static int launch_group(mpb_batch_plan *pl, int g, cudaStream_t st) {
   if (pl->gcount[g] == 0 || pl->gunits[g] == 0) return MPB_OK;
-  KernelFn fn = kernel_of(g);
   const Tuning t = pl->tune[g];
+  size_t smem = 0;
+  KernelFn fn = t.lanes > 1 ? coop_kernel_of(g, t.lanes, t.block, &smem) : kernel_of(g);
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, t.block, 0) != cudaSuccess || per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, t.block, smem) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   const int bps = t.blocks_per_sm > 0 ? std::min(t.blocks_per_sm, per_sm) : per_sm;
   long long grid = (long long)sm_count() * bps;
   const long long warps_needed = pl->gunits[g];
   const long long max_grid = (warps_needed * 32 + t.block - 1) / t.block;
   grid = std::min(grid, std::max(1LL, max_grid));
-  fn<<<(int)grid, t.block, 0, st>>>(pl->probs, pl->order + pl->gstart[g], pl->prefix + pl->gstart[g], pl->gcount[g],
-                                    pl->gunits[g], (unsigned long long *)((uint8_t *)pl->counters + 64 * g));
+  fn<<<(int)grid, t.block, smem, st>>>(pl->probs, pl->order + pl->gstart[g], pl->prefix + pl->gstart[g],
+                                       pl->gcount[g], pl->gunits[g],
+                                       (unsigned long long *)((uint8_t *)pl->counters + 64 * g));
   return launch_status();
 }
 
@@ -277,7 +341,14 @@ extern "C" int mpb_batch_gemv_autotune(mpb_batch_plan *pl, void *stream) {
     if (pl->gcount[g] == 0) continue;
     float best = 1e30f;
     Tuning bestt = pl->tune[g];
-    for (const Tuning &c : kCandidates) {
+    std::vector<Tuning> cands(std::begin(kCandidates), std::end(kCandidates));
+    for (int lanes : {4, 8, 16})
+      if (lanes_ok(g, lanes))
+        for (Tuning c : kCoopCandidates) {
+          c.lanes = lanes;
+          cands.push_back(c);
+        }
+    for (const Tuning &c : cands) {
       pl->tune[g] = c;
       float ms_sum = 0.0f;
       for (int rep = 0; rep < 3 && rc == MPB_OK; ++rep) {
@@ -325,7 +396,25 @@ extern "C" int mpb_batch_gemv_set_tuning(mpb_batch_plan *pl, int prec, int block
   const int g = group_of(prec);
   if (g < 0) return MPB_ERR_PREC;
   if (block < 32 || block > 256 || block % 32 != 0 || blocks_per_sm < 0 || blocks_per_sm > 64) return MPB_ERR_ARG;
-  pl->tune[g] = Tuning{block, blocks_per_sm};
+  pl->tune[g].block = block;
+  pl->tune[g].blocks_per_sm = blocks_per_sm;
+  return MPB_OK;
+}
+
+extern "C" int mpb_batch_gemv_get_split(const mpb_batch_plan *pl, int prec, int *lanes) {
+  if (!pl || !lanes) return MPB_ERR_NULL;
+  const int g = group_of(prec);
+  if (g < 0) return MPB_ERR_PREC;
+  *lanes = pl->tune[g].lanes;
+  return MPB_OK;
+}
+
+extern "C" int mpb_batch_gemv_set_split(mpb_batch_plan *pl, int prec, int lanes) {
+  if (!pl) return MPB_ERR_NULL;
+  const int g = group_of(prec);
+  if (g < 0) return MPB_ERR_PREC;
+  if (!lanes_ok(g, lanes)) return MPB_ERR_ARG;
+  pl->tune[g].lanes = lanes;
   return MPB_OK;
 }
 

@@ -52,7 +52,69 @@ void profile_mark(int phase, bool begin, cudaStream_t st) {
     g_iv[phase].emplace_back(g_open[phase], e), g_open[phase] = nullptr;
 }
 
+/* ---------------- thread-vs-warp split ---------------- */
+/* lanes per element of the kernels that have a warp-cooperative form, per
+ * kind and precision group (64 .. 2048); 1 = one thread per element */
+static std::atomic<int> g_split[kSplitKinds][6];
+static std::once_flag g_split_once;
+
+static int prec_group(int prec) {
+  switch (prec) {
+    case 64: return 0;
+    case 128: return 1;
+    case 256: return 2;
+    case 512: return 3;
+    case 1024: return 4;
+    case 2048: return 5;
+    default: return -1;
+  }
+}
+
+bool split_supported(int kind, int prec, int lanes) {
+  if (kind < 0 || kind >= kSplitKinds || prec_group(prec) < 0) return false;
+  if (lanes == 1) return true;
+  if (kind == MPB_SPLIT_AXPY_C) return prec == 1024 && (lanes == 4 || lanes == 8);
+  if (prec == 1024) return lanes == 4 || lanes == 8;
+  if (prec == 2048) return lanes == 8 || lanes == 16;
+  return false;
+}
+
+static void split_defaults() {
+  for (int k = 0; k < kSplitKinds; ++k)
+    for (int g = 0; g < 6; ++g) g_split[k][g].store(1, std::memory_order_relaxed);
+  /* measured on B200: the cooperative forms win from 1024 bits on */
+  g_split[MPB_SPLIT_GEMV_R][4].store(kDefaultSplit1024, std::memory_order_relaxed);
+  g_split[MPB_SPLIT_GEMV_R][5].store(kDefaultSplit2048, std::memory_order_relaxed);
+  g_split[MPB_SPLIT_AXPY_C][4].store(kDefaultSplitAxpyC1024, std::memory_order_relaxed);
+}
+
+int split_lanes(int kind, int prec) {
+  std::call_once(g_split_once, split_defaults);
+  const int g = prec_group(prec);
+  if (kind < 0 || kind >= kSplitKinds || g < 0) return 1;
+  return g_split[kind][g].load(std::memory_order_relaxed);
+}
+
 } /* namespace mpb */
+
+extern "C" int mpb_set_split(int kind, int prec, int lanes) {
+  using namespace mpb;
+  if (kind < 0 || kind >= kSplitKinds) return MPB_ERR_ARG;
+  if (prec_group(prec) < 0) return MPB_ERR_PREC;
+  if (!split_supported(kind, prec, lanes)) return MPB_ERR_ARG;
+  std::call_once(g_split_once, split_defaults);
+  g_split[kind][prec_group(prec)].store(lanes, std::memory_order_relaxed);
+  return MPB_OK;
+}
+
+extern "C" int mpb_get_split(int kind, int prec, int *lanes) {
+  using namespace mpb;
+  if (!lanes) return MPB_ERR_NULL;
+  if (kind < 0 || kind >= kSplitKinds) return MPB_ERR_ARG;
+  if (prec_group(prec) < 0) return MPB_ERR_PREC;
+  *lanes = split_lanes(kind, prec);
+  return MPB_OK;
+}
 
 extern "C" void mpb_profile_enable(int on) {
   using namespace mpb;

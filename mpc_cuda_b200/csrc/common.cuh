@@ -36,6 +36,15 @@ inline int launch_status() {
 /* SM count of the current device (cached per device) */
 int sm_count();
 
+/* thread-vs-warp split (mpb_set_split): lanes per element for a kind and
+ * precision, 1 = one thread per element */
+constexpr int kSplitKinds = 2;
+constexpr int kDefaultSplit1024 = 8;      /* GEMV rows at 1024 bits */
+constexpr int kDefaultSplit2048 = 8;      /* GEMV rows at 2048 bits */
+constexpr int kDefaultSplitAxpyC1024 = 1; /* complex AXPY elements at 1024 bits */
+int split_lanes(int kind, int prec);
+bool split_supported(int kind, int prec, int lanes);
+
 /* Opt-in phase timing (mpb_profile_enable): entry points that run several
  * kernels record a CUDA event pair around each phase on the caller's stream. */
 enum {

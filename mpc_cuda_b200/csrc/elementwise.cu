@@ -11,6 +11,7 @@
 #include <initializer_list>
 
 #include "common.cuh"
+#include "mpb/coop.cuh"
 
 namespace mpb {
 
@@ -255,6 +256,48 @@ __global__ void __launch_bounds__(kBlock) k_axpy_c(size_t n, const uint8_t *a, c
   }
 }
 
+/* complex AXPY with a group of G lanes per element (the warp-cooperative form
+ * for wide operands): both components of a*x from the exact products, one
+ * rounding each (coop::fmms_u, the scalar's parts as the uniform operands),
+ * then the rounded adds of y, as k_axpy_c */
+template <int L, int G>
+__global__ void __launch_bounds__(kBlock) k_axpy_c_coop(size_t n, const uint8_t *a, const uint8_t *x, const uint8_t *y,
+                                                        uint8_t *z) {
+  constexpr int N = G * L, EPW = 32 / G, SMW = 6 * N + 3;
+  constexpr size_t TB = sol<N>::kTileBytes;
+  __shared__ uint32_t sm_all[(kBlock / 32) * EPW * SMW];
+  const uint32_t warp = threadIdx.x >> 5, gw = (threadIdx.x & 31u) / G;
+  uint32_t *sm = sm_all + (warp * EPW + gw) * SMW;
+  const coop::uref ar{a, 0u}, ai{a + TB, 0u}; /* element 0: re tile, then im tile */
+  int32_t are, aie;
+  uint32_t ars, ais;
+  coop::uniform_head<N>(ar, are, ars);
+  coop::uniform_head<N>(ai, aie, ais);
+  const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const size_t egroups = (n + EPW - 1) / EPW;
+  for (size_t eg = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; eg < egroups; eg += nw) {
+    const size_t i = eg * EPW + gw;
+    const size_t ic = i < n ? i : n - 1; /* lanes past the end recompute the last element */
+    const uint8_t *xt = x + (ic >> 5) * 2u * TB;
+    const uint8_t *yt = y + (ic >> 5) * 2u * TB;
+    const uint32_t slot = (uint32_t)(ic & 31u);
+    coop::cv<L> xr, xi, yv, re, im;
+    coop::load<L, G, kStream>(xr, xt, slot);
+    coop::load<L, G, kStream>(xi, xt + TB, slot);
+    coop::fmms_u<L, G>(re, xr, ar, are, ars, xi, ai, aie, ais, 1u, sm); /* xr ar - xi ai */
+    coop::fmms_u<L, G>(im, xr, ai, aie, ais, xi, ar, are, ars, 0u, sm); /* xr ai + xi ar */
+    coop::load<L, G, kStream>(yv, yt, slot);
+    coop::add<L, G>(re, re, yv, sm);
+    coop::load<L, G, kStream>(yv, yt + TB, slot);
+    coop::add<L, G>(im, im, yv, sm);
+    if (i < n) {
+      uint8_t *zt = z + (i >> 5) * 2u * TB;
+      coop::store<L, G, kStream>(zt, slot, re);
+      coop::store<L, G, kStream>(zt + TB, slot, im);
+    }
+  }
+}
+
 } /* namespace mpb */
 
 using namespace mpb;
@@ -389,6 +432,20 @@ extern "C" int mpb_axpy_r(int prec, size_t n, const void *a, const void *x, cons
 extern "C" int mpb_axpy_c(int prec, size_t n, const void *a, const void *x, const void *y, void *z, void *stream) {
   const int rc = vec_args(prec, n, {a, x, y, z});
   if (rc != MPB_OK) return rc > 0 ? MPB_OK : rc;
+  const int lanes = split_lanes(MPB_SPLIT_AXPY_C, prec);
+  if (prec == 1024 && lanes > 1) {
+    const size_t warps = (n + 32 / lanes - 1) / (32 / lanes);
+    if (lanes == 4) {
+      const int g = grid_for(k_axpy_c_coop<8, 4>, kBlock, warps * 32u);
+      k_axpy_c_coop<8, 4><<<g, kBlock, 0, as_stream(stream)>>>(n, (const uint8_t *)a, (const uint8_t *)x,
+                                                              (const uint8_t *)y, (uint8_t *)z);
+    } else {
+      const int g = grid_for(k_axpy_c_coop<4, 8>, kBlock, warps * 32u);
+      k_axpy_c_coop<4, 8><<<g, kBlock, 0, as_stream(stream)>>>(n, (const uint8_t *)a, (const uint8_t *)x,
+                                                              (const uint8_t *)y, (uint8_t *)z);
+    }
+    return launch_status();
+  }
   MPB_DISPATCH_PREC(prec, {
     const int g = grid_for(k_axpy_c<N>, kBlock, tiles_for(n) * 32u);
     k_axpy_c<N><<<g, kBlock, 0, as_stream(stream)>>>(n, (const uint8_t *)a, (const uint8_t *)x, (const uint8_t *)y,

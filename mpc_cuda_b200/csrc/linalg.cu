@@ -14,6 +14,7 @@
 #include <initializer_list>
 
 #include "common.cuh"
+#include "coop_rows.cuh"
 
 namespace mpb {
 
@@ -83,6 +84,26 @@ __global__ void __launch_bounds__(kGemvBlock) k_gemv_r(size_t m, size_t n, const
   }
 }
 
+/* GEMV with a group of G lanes per row (the warp-cooperative form for wide
+ * operands): the warps of the grid stride over groups of 32/G rows */
+template <int L, int G>
+__global__ void __launch_bounds__(kGemvBlock) k_gemv_r_coop(size_t m, size_t n, const uint8_t *A, size_t lda,
+                                                            const uint8_t *x, const uint8_t *y, uint8_t *yo) {
+  constexpr int N = G * L, RPW = 32 / G, SMW = coop_row_smem<N>::words;
+  __shared__ uint32_t sm_all[(kGemvBlock / 32) * RPW * SMW];
+  const uint32_t warp = threadIdx.x >> 5, gw = (threadIdx.x & 31u) / G;
+  uint32_t *sm = sm_all + (warp * RPW + gw) * SMW;
+  const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const size_t rgroups = (m + RPW - 1) / RPW;
+  for (size_t rg = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; rg < rgroups; rg += nw) {
+    const size_t i = rg * RPW + gw;
+    const size_t ir = i < m ? i : m - 1; /* lanes past the last row recompute it */
+    coop::cv<L> acc;
+    coop_gemv_row<L, G>(acc, A, ir * lda, n, x, y, ir, sm);
+    if (i < m) coop::store<L, G>(yo, i, acc);
+  }
+}
+
 template <int N>
 __global__ void __launch_bounds__(kGemvBlock) k_gemv_c(size_t m, size_t n, const uint8_t *A, size_t lda,
                                                        const uint8_t *x, const uint8_t *y, uint8_t *yo) {
@@ -128,6 +149,31 @@ static int bufs_ok(std::initializer_list<const void *> bufs) {
 
 using namespace mpb;
 
+template <int L, int G>
+static void launch_gemv_coop_lg(size_t m, size_t n, const uint8_t *A, size_t lda, const uint8_t *x, const uint8_t *y,
+                                uint8_t *yo, cudaStream_t st) {
+  const size_t warps = (m + 32 / G - 1) / (32 / G);
+  const int g = grid_for(k_gemv_r_coop<L, G>, kGemvBlock, warps * 32u);
+  k_gemv_r_coop<L, G><<<g, kGemvBlock, 0, st>>>(m, n, A, lda, x, y, yo);
+}
+/* the cooperative GEMV at N limbs with `lanes` lanes per row (1024 bits: 4 or
+ * 8 lanes, 2048 bits: 8 or 16; mpb_set_split validates) */
+template <int N>
+static void launch_gemv_coop(int lanes, size_t m, size_t n, const uint8_t *A, size_t lda, const uint8_t *x,
+                             const uint8_t *y, uint8_t *yo, cudaStream_t st) {
+  if constexpr (N == 32) {
+    if (lanes == 4)
+      launch_gemv_coop_lg<8, 4>(m, n, A, lda, x, y, yo, st);
+    else
+      launch_gemv_coop_lg<4, 8>(m, n, A, lda, x, y, yo, st);
+  } else if constexpr (N == 64) {
+    if (lanes == 8)
+      launch_gemv_coop_lg<8, 8>(m, n, A, lda, x, y, yo, st);
+    else
+      launch_gemv_coop_lg<4, 16>(m, n, A, lda, x, y, yo, st);
+  }
+}
+
 template <bool CPLX>
 static int gemv_entry(int prec, size_t m, size_t n, const void *A, size_t lda, const void *x, const void *y,
                       void *yo, void *stream) {
@@ -151,6 +197,9 @@ static int gemv_entry(int prec, size_t m, size_t n, const void *A, size_t lda, c
       const int g = grid_for(k_gemv_c<N>, kGemvBlock, tiles_for(m) * 32u);
       k_gemv_c<N><<<g, kGemvBlock, 0, as_stream(stream)>>>(m, n, (const uint8_t *)A, lda, (const uint8_t *)x,
                                                             (const uint8_t *)y, (uint8_t *)yo);
+    } else if (N >= 32 && split_lanes(MPB_SPLIT_GEMV_R, prec) > 1) {
+      launch_gemv_coop<N>(split_lanes(MPB_SPLIT_GEMV_R, prec), m, n, (const uint8_t *)A, lda, (const uint8_t *)x,
+                          (const uint8_t *)y, (uint8_t *)yo, as_stream(stream));
     } else {
       const int g = grid_for(k_gemv_r<N>, kGemvBlock, tiles_for(m) * 32u);
       k_gemv_r<N><<<g, kGemvBlock, 0, as_stream(stream)>>>(m, n, (const uint8_t *)A, lda, (const uint8_t *)x,
