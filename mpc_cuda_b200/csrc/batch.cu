@@ -102,8 +102,12 @@ __global__ void __launch_bounds__(256) k_batch_gemv(const DevProb *probs, const 
   }
 }
 
-/* the same with G lanes per row: a warp takes a 32-row unit and runs it as G
- * passes of 32/G rows (passes past the problem's last row are skipped) */
+/* the same with G lanes per row.  A 32-row unit is split into G work items
+ * of 32/G rows (nunits counts the items: G per unit), each taken by one warp:
+ * the rows of a long problem then run on G times as many warps at once, and
+ * the batch's critical path -- the longest row's sequential k loop -- is the
+ * cooperative row's, a fraction of one thread's (items past a problem's last
+ * row return at once) */
 template <int L, int G>
 __global__ void __launch_bounds__(256) k_batch_gemv_coop(const DevProb *probs, const int *order,
                                                          const long long *prefix, int nprob, long long nunits,
@@ -118,19 +122,21 @@ __global__ void __launch_bounds__(256) k_batch_gemv_coop(const DevProb *probs, c
     if (lane == 0) u = (long long)atomicAdd(counter, 1ull);
     u = __shfl_sync(0xffffffffu, u, 0);
     if (u >= nunits) break;
+    const long long unit = u / G;
+    const int pass = (int)(u % G);
     int lo = 0, hi = nprob - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (prefix[mid] <= u)
+      if (prefix[mid] <= unit)
         lo = mid;
       else
         hi = mid - 1;
     }
     const DevProb pr = probs[order[lo]];
-    const long long blk = u - prefix[lo];
-    for (int pass = 0; pass < G; ++pass) {
+    const long long blk = unit - prefix[lo];
+    {
       const int r0 = (int)(blk * 32) + pass * RPW;
-      if (r0 >= pr.m) break; /* warp-uniform */
+      if (r0 >= pr.m) continue; /* warp-uniform: an item past the last row */
       const int i = r0 + (int)gw;
       const int ir = i < pr.m ? i : pr.m - 1;
       coop::cv<L> acc;
@@ -311,11 +317,11 @@ static int launch_group(mpb_batch_plan *pl, int g, cudaStream_t st) {
     per_sm = 1;
   const int bps = t.blocks_per_sm > 0 ? std::min(t.blocks_per_sm, per_sm) : per_sm;
   long long grid = (long long)sm_count() * bps;
-  const long long warps_needed = pl->gunits[g];
-  const long long max_grid = (warps_needed * 32 + t.block - 1) / t.block;
+  const long long items = pl->gunits[g] * (t.lanes > 1 ? t.lanes : 1); /* one warp per item */
+  const long long max_grid = (items * 32 + t.block - 1) / t.block;
   grid = std::min(grid, std::max(1LL, max_grid));
   fn<<<(int)grid, t.block, smem, st>>>(pl->probs, pl->order + pl->gstart[g], pl->prefix + pl->gstart[g],
-                                       pl->gcount[g], pl->gunits[g],
+                                       pl->gcount[g], items,
                                        (unsigned long long *)((uint8_t *)pl->counters + 64 * g));
   return launch_status();
 }
