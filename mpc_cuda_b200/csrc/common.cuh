@@ -7,6 +7,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "mpb.h"
 #include "mpb/layout.cuh"
 
@@ -35,6 +37,34 @@ inline int launch_status() {
 
 /* SM count of the current device (cached per device) */
 int sm_count();
+
+/* Programmatic dependent launch: a kernel launched with launch_pdl may start
+ * (be scheduled, run its prologue) while the kernel before it on the stream
+ * is finishing; it must call pdl_wait() before it touches memory that kernel
+ * writes.  pdl_wait() waits for the whole previous grid and the visibility of
+ * its writes; in a kernel launched normally it returns at once.  Used along
+ * the chains of small dependent launches, where it hides the launch latency
+ * between them. */
+__device__ __forceinline__ void pdl_wait() {
+#if defined(__CUDA_ARCH__)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 /* thread-vs-warp split (mpb_set_split): lanes per element for a kind and
  * precision, 1 = one thread per element */

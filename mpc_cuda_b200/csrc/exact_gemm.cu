@@ -96,6 +96,7 @@ __device__ __forceinline__ Unit decode(const GemmArgs &g, long u, long T) {
 
 __global__ void __launch_bounds__(kGemmThreads, 1)
     k_diag_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g) {
+  pdl_wait(); /* launched after the previous stage with launch_pdl */
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t *sA = smem;
@@ -341,8 +342,9 @@ int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *e
   const long grid = std::min<long>(ga.units, (long)sm_count());
   const int phase = tiles ? kPhaseTensorLow : kPhaseTensor;
   profile_mark(phase, true, st);
-  k_diag_gemm<<<(int)grid, kGemmThreads, kSmemBytes, st>>>(tmA, tmB, ga);
+  const cudaError_t e = launch_pdl(k_diag_gemm, dim3((unsigned)grid), dim3(kGemmThreads), kSmemBytes, st, tmA, tmB, ga);
   profile_mark(phase, false, st);
+  if (e != cudaSuccess) return MPB_ERR_CUDA;
   return launch_status();
 }
 

@@ -163,6 +163,7 @@ constexpr int32_t kColMinNone = (int32_t)0x7f7f7f7f; /* memset 0x7f */
 template <int N, bool CPLX>
 __global__ void __launch_bounds__(256) k_col_stats(int n, int k, const uint8_t *B, size_t ldb, int32_t *colE,
                                                    int32_t *colEmin) {
+  pdl_wait(); /* launched after the previous stage with launch_pdl */
   __shared__ int32_t smax[8][32], smin[8][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int j = blockIdx.x * 32 + lane;
@@ -205,6 +206,7 @@ template <int N, bool CPLX>
 __global__ void __launch_bounds__(256) k_row_stats(int m, int k, const uint8_t *A, size_t lda, int SP, int32_t *rowE,
                                                    uint8_t *rowF, int n, int32_t *colE, const int32_t *colEmin,
                                                    uint8_t *colF, int *count) {
+  pdl_wait(); /* launched after the previous stage with launch_pdl */
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const int32_t e = colE[j];
     const bool none = e == kColNone;
@@ -322,6 +324,7 @@ __device__ __forceinline__ void element_digits(const fval<N> &re, const fval<N> 
 template <int N, int XL, bool CPLX>
 __global__ void __launch_bounds__(128) k_slice_a(int m, int k, int kp, const uint8_t *A, size_t lda, int SP, int S,
                                                  const int32_t *rowE, const uint8_t *rowF, int8_t *Asl) {
+  pdl_wait(); /* launched after the previous stage with launch_pdl */
   const size_t total = (size_t)m * kp, plane = (size_t)m * kp;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (size_t)gridDim.x * blockDim.x) {
@@ -350,6 +353,7 @@ __global__ void __launch_bounds__(128) k_slice_a(int m, int k, int kp, const uin
 template <int N, int XL, bool CPLX>
 __global__ void __launch_bounds__(128) k_slice_b(int n, int k, int kp, const uint8_t *B, size_t ldb, int SP, int S,
                                                  const int32_t *colE, const uint8_t *colF, int8_t *Bsl) {
+  pdl_wait(); /* launched after the previous stage with launch_pdl */
   const size_t total = (size_t)n * kp, plane = (size_t)n * kp;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (size_t)gridDim.x * blockDim.x) {
@@ -613,6 +617,7 @@ __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
                                   round_geo<N, XL>::template threads<CPLX>() == 128 ? 4 : 8)
     k_exact_round(int m, int n, int S, int SP, const int32_t *__restrict__ D, const int32_t *rowE, const int32_t *colE,
                   const uint8_t *rowF, const uint8_t *colF, uint8_t *C, size_t ldc, RoundPass rp) {
+  pdl_wait(); /* launched after the previous stage with launch_pdl */
   constexpr int J = round_geo<N, XL>::J;
   constexpr int QJ = round_geo<N, XL>::QJ;
   constexpr int SW = QJ | 1; /* odd word stride per thread: conflict-free banks */
@@ -713,6 +718,7 @@ __global__ void __launch_bounds__(128) k_exact_round_parts(int m, int n, int S, 
                                                            const int32_t *rowE, const int32_t *colE,
                                                            const uint8_t *rowF, const uint8_t *colF, uint8_t *C,
                                                            size_t ldc, RoundPass rp) {
+  pdl_wait(); /* launched after the previous stage with launch_pdl */
   constexpr int Q = round_geo<N, XL>::Q;
   const size_t total = pass_total(rp, m, n), plane = rp.dplane;
   const int ndiag = 2 * S - 1;
@@ -778,7 +784,13 @@ __global__ void __launch_bounds__(128) k_exact_round_parts(int m, int n, int S, 
 template <int N, bool CPLX>
 __global__ void __launch_bounds__(256) k_fallback(size_t m, size_t n, size_t K, const uint8_t *A, size_t lda,
                                                   const uint8_t *B, size_t ldb, uint8_t *C, size_t ldc,
-                                                  const uint8_t *rowF, const uint8_t *colF) {
+                                                  const uint8_t *rowF, const uint8_t *colF, const int *cnt,
+                                                  int *status) {
+  pdl_wait(); /* launched after the previous stage with launch_pdl */
+  if (status && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    status[0] = cnt[0]; /* fallback rows + columns, counted by k_row_stats */
+    status[1] = cnt[1]; /* error code of the tensor-core launches */
+  }
   const size_t i = (size_t)blockIdx.y * 8 + (threadIdx.x >> 5);
   const size_t j = (size_t)blockIdx.x * 32u + (threadIdx.x & 31u);
   if (i >= m || j >= n) return;
@@ -810,6 +822,21 @@ __global__ void __launch_bounds__(256) k_fallback(size_t m, size_t n, size_t K, 
   }
 }
 
+/* the counters and column statistics every call starts from (one launch in
+ * place of four memsets, so the whole chain is kernel to kernel) */
+static __global__ void __launch_bounds__(256) k_exact_init(int *cnt, int *tf, size_t ntf, int32_t *colE, int32_t *colEmin,
+                                                   size_t n) {
+  pdl_wait();
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t0 < 4) cnt[t0] = 0;
+  for (size_t i = t0; i < ntf; i += stride) tf[i] = 0;
+  for (size_t j = t0; j < n; j += stride) {
+    colE[j] = kColNone;
+    colEmin[j] = kColMinNone;
+  }
+}
+
 template <int N, int XL, bool CPLX>
 static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *B, size_t ldb, uint8_t *C,
                     size_t ldc, uint8_t *ws, int *n_fallback, cudaStream_t st) {
@@ -828,33 +855,32 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
   rp.tf = (int *)(ws + p.off_tf);
   rp.tiles = (int *)(ws + p.off_tiles);
   rp.ntiles = cnt + 2;
-  if (cudaMemsetAsync(cnt, 0, 16, st) != cudaSuccess ||
-      cudaMemsetAsync(rp.tf, 0, 4 * (size_t)p.mt * p.nt, st) != cudaSuccess)
-    return MPB_ERR_CUDA;
-
+  /* every stage after the first is launched with launch_pdl: it is scheduled
+   * while the previous one finishes and waits for it in pdl_wait() */
   int32_t *colEmin = (int32_t *)(ws + p.off_colEmin);
-  if (cudaMemsetAsync(colE, 0x80, 4 * (size_t)p.n, st) != cudaSuccess ||
-      cudaMemsetAsync(colEmin, 0x7f, 4 * (size_t)p.n, st) != cudaSuccess)
-    return MPB_ERR_CUDA;
-  profile_mark(kPhaseStats, true, st);
   {
-    const dim3 grid((p.n + 31) / 32, (p.k + kColRows - 1) / kColRows);
-    k_col_stats<N, CPLX><<<grid, 256, 0, st>>>(p.n, p.k, B, ldb, colE, colEmin);
+    const size_t ntf = (size_t)p.mt * p.nt, most = ntf > (size_t)p.n ? ntf : (size_t)p.n;
+    const int g = (int)std::min<size_t>((most + 255) / 256 + 1, (size_t)4 * sm_count());
+    k_exact_init<<<g, 256, 0, st>>>(cnt, rp.tf, ntf, colE, colEmin, (size_t)p.n);
   }
-  k_row_stats<N, CPLX><<<(p.m + 7) / 8, 256, 0, st>>>(p.m, p.k, A, lda, p.SP, rowE, rowF, p.n, colE, colEmin, colF,
-                                                      cnt);
+  if (launch_status() != MPB_OK) return MPB_ERR_CUDA;
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t r) {
+    if (r != cudaSuccess && e == cudaSuccess) e = r;
+  };
+  profile_mark(kPhaseStats, true, st);
+  chk(launch_pdl(k_col_stats<N, CPLX>, dim3((p.n + 31) / 32, (p.k + kColRows - 1) / kColRows), dim3(256), 0, st,
+                 p.n, p.k, B, ldb, colE, colEmin));
+  chk(launch_pdl(k_row_stats<N, CPLX>, dim3((p.m + 7) / 8), dim3(256), 0, st, p.m, p.k, A, lda, p.SP, rowE, rowF,
+                 p.n, colE, (const int32_t *)colEmin, colF, cnt));
   profile_mark(kPhaseStats, false, st);
   profile_mark(kPhaseSlice, true, st);
-  {
-    const int g = grid_for(k_slice_a<N, XL, CPLX>, 128, (size_t)p.m * p.kp);
-    k_slice_a<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.k, p.kp, A, lda, p.SP, p.S, rowE, rowF, Asl);
-  }
-  {
-    const int g = grid_for(k_slice_b<N, XL, CPLX>, 128, (size_t)p.n * p.kp);
-    k_slice_b<N, XL, CPLX><<<g, 128, 0, st>>>(p.n, p.k, p.kp, B, ldb, p.SP, p.S, colE, colF, Bsl);
-  }
+  chk(launch_pdl(k_slice_a<N, XL, CPLX>, dim3(grid_for(k_slice_a<N, XL, CPLX>, 128, (size_t)p.m * p.kp)), dim3(128),
+                 0, st, p.m, p.k, p.kp, A, lda, p.SP, p.S, (const int32_t *)rowE, (const uint8_t *)rowF, Asl));
+  chk(launch_pdl(k_slice_b<N, XL, CPLX>, dim3(grid_for(k_slice_b<N, XL, CPLX>, 128, (size_t)p.n * p.kp)), dim3(128),
+                 0, st, p.n, p.k, p.kp, B, ldb, p.SP, p.S, (const int32_t *)colE, (const uint8_t *)colF, Bsl));
   profile_mark(kPhaseSlice, false, st);
-  if (launch_status() != MPB_OK) return MPB_ERR_CUDA;
+  if (e != cudaSuccess || launch_status() != MPB_OK) return MPB_ERR_CUDA;
 
   /* main pass: diagonals [d0, 2S-2] of every tile */
   {
@@ -862,14 +888,17 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
     if (rc != MPB_OK) return rc;
   }
   auto round_pass = [&](const RoundPass &r, int grid_cap) {
+    const int32_t *Dc = D, *rE = rowE, *cE = colE;
+    const uint8_t *rF = rowF, *cF = colF;
     if (p.P == 1 && !r.flagged_only && 2 * p.S - 1 - r.d_first <= round_geo<N, XL>::J) {
       constexpr int T = round_geo<N, XL>::template threads<CPLX>();
       const int g = std::min(grid_cap, grid_for(k_exact_round<N, XL, CPLX>, T, (size_t)p.m * p.n));
-      k_exact_round<N, XL, CPLX><<<g, T, 0, st>>>(p.m, p.n, p.S, p.SP, D, rowE, colE, rowF, colF, C, ldc, r);
+      chk(launch_pdl(k_exact_round<N, XL, CPLX>, dim3(g), dim3(T), 0, st, p.m, p.n, p.S, p.SP, Dc, rE, cE, rF, cF,
+                     C, ldc, r));
     } else {
       const int g = std::min(grid_cap, grid_for(k_exact_round_parts<N, XL, CPLX>, 128, (size_t)p.m * p.n));
-      k_exact_round_parts<N, XL, CPLX><<<g, 128, 0, st>>>(p.m, p.n, p.S, p.SP, p.P, D, rowE, colE, rowF, colF, C,
-                                                          ldc, r);
+      chk(launch_pdl(k_exact_round_parts<N, XL, CPLX>, dim3(g), dim3(128), 0, st, p.m, p.n, p.S, p.SP, p.P, Dc, rE,
+                     cE, rF, cF, C, ldc, r));
     }
   };
   profile_mark(kPhaseRound, true, st);
@@ -888,13 +917,11 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
     round_pass(r2, 4 * sm_count());
   }
   profile_mark(kPhaseFallback, true, st);
-  {
-    const dim3 grid((p.n + 31) / 32, (p.m + 7) / 8);
-    k_fallback<N, CPLX><<<grid, 256, 0, st>>>(p.m, p.n, p.k, A, lda, B, ldb, C, ldc, rowF, colF);
-  }
+  chk(launch_pdl(k_fallback<N, CPLX>, dim3((p.n + 31) / 32, (p.m + 7) / 8), dim3(256), 0, st, (size_t)p.m,
+                 (size_t)p.n, (size_t)p.k, A, lda, B, ldb, C, ldc, (const uint8_t *)rowF, (const uint8_t *)colF,
+                 (const int *)cnt, n_fallback));
   profile_mark(kPhaseFallback, false, st);
-  if (n_fallback && cudaMemcpyAsync(n_fallback, cnt, 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-    return MPB_ERR_CUDA;
+  if (e != cudaSuccess) return MPB_ERR_CUDA;
   return launch_status();
 }
 
