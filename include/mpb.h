@@ -90,6 +90,21 @@ int mpb_cunpack_aos(int prec, size_t n, const void *cvec, void *aos, void *strea
 enum { MPB_RP_MUL = 0, MPB_RP_ADD = 1, MPB_RP_SUB = 2, MPB_RP_FMA = 3, MPB_RP_DIV = 4, MPB_RP_SQRT = 5 };
 int mpb_storage_prec(int prec); /* PB, or MPB_ERR_PREC */
 int mpb_op_rp(int op, int prec, size_t n, const void *a, const void *b, const void *c, void *r, void *stream);
+/* AXPY, GEMV and GEMM at a runtime precision prec (1 .. 2046 bits), every
+ * operation correctly rounded at prec bits in the order of mpb_axpy_r /
+ * mpb_gemv_r / mpb_gemm_r (MPFR with prec-bit destinations; the reference's
+ * runtime layer takes its precision per call, src/mpfr_cuda/mpfr.h:582-589);
+ * vectors in the layout of the storage precision mpb_storage_prec(prec). */
+int mpb_axpy_r_rp(int prec, size_t n, const void *a, const void *x, const void *y, void *z, void *stream);
+int mpb_gemv_r_rp(int prec, size_t m, size_t n, const void *A, size_t lda, const void *x, const void *y,
+                  void *y_out, void *stream);
+int mpb_gemm_r_rp(int prec, size_t m, size_t n, size_t k, const void *A, size_t lda, const void *B, size_t ldb,
+                  void *C, size_t ldc, void *stream);
+/* an elementary function (MPB_FN_*) at a runtime precision: faithful at the
+ * storage precision, then rounded to nearest at prec bits, so within 1 ULP of
+ * prec bits (the faithful contract of the reference's cu_fmath functions at a
+ * precision chosen per call) */
+int mpb_fmath_r_rp(int fn, int prec, size_t n, const void *a, const void *b, void *r, void *stream);
 
 /* ---- host interop with MPFR / MPC objects (host memory, no GPU, no MPFR link) ----
  * dst[i] / src[i] point to initialised mpfr_t (mpfr_ptr) or mpc_t objects; AoS
@@ -298,6 +313,15 @@ int mpb_gemm_exact_c(int prec, size_t m, size_t n, size_t k, const void *A, size
  * tensor-core work is 2 * pairs * m * n * k per real product). */
 int mpb_gemm_exact_plan_info(int prec, size_t m, size_t n, size_t k, int sp_bits, int cplx, int *slices,
                              int *first_diag, long long *pairs);
+/* Test of the failure path (no counterpart in the reference): the next
+ * tensor-core launch of an exact GEMM in this process runs with one
+ * accumulator commit withheld in its first CTA and every barrier wait limited
+ * to wait_ns nanoseconds (1e3 .. 2e9), so that CTA's wait runs out.  The
+ * kernel then raises its abort flag, records an error code (1-4) in the
+ * call's status[1], waits for its own MMAs and copies, frees its tensor
+ * memory and returns: the results of that call are not valid, and the next
+ * call on the same stream is correct again.  what: 1.  MPB_ERR_ARG otherwise. */
+int mpb_gemm_exact_test_inject(int what, long long wait_ns);
 /* The same exact GEMM for callers that cannot allocate device memory (a
  * latency-critical loop that must not call cudaMalloc after start-up, or a
  * framework that owns the whole memory pool): no workspace argument and no

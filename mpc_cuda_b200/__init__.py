@@ -101,6 +101,11 @@ _SIGS = {
     "mpb_gemm_exact_c_workspace": ([_I, _S, _S, _S, _I], C.c_size_t),
     "mpb_gemm_exact_c": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _I, _V, _S, _V, _V], C.c_int),
     "mpb_gemm_exact_r_static": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _I, _V, _V], C.c_int),
+    "mpb_gemm_exact_test_inject": ([_I, C.c_longlong], C.c_int),
+    "mpb_axpy_r_rp": ([_I, _S, _V, _V, _V, _V, _V], C.c_int),
+    "mpb_gemv_r_rp": ([_I, _S, _S, _V, _S, _V, _V, _V, _V], C.c_int),
+    "mpb_gemm_r_rp": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _V], C.c_int),
+    "mpb_fmath_r_rp": ([_I, _I, _S, _V, _V, _V, _V], C.c_int),
 }
 
 
@@ -291,6 +296,24 @@ def op_rp(op, prec, n, a, r, b=None, c=None, stream=None):
     """r = op(a, b, c) correctly rounded at a runtime precision prec (vectors in
     the storage_prec(prec) format); op in RP_OPS."""
     _call("mpb_op_rp", RP_OPS.index(op), prec, n, _ptr(a), _ptr(b), _ptr(c), _ptr(r), _stream(stream))
+
+
+def axpy_rp(prec, n, a, x, y, z, stream=None):
+    """z = round(round(a*x) + y) at a runtime precision prec (storage_prec layout)."""
+    _call("mpb_axpy_r_rp", prec, n, _ptr(a), _ptr(x), _ptr(y), _ptr(z), _stream(stream))
+
+
+def gemv_rp(prec, m, n, A, lda, x, y, y_out, stream=None):
+    _call("mpb_gemv_r_rp", prec, m, n, _ptr(A), lda, _ptr(x), _ptr(y), _ptr(y_out), _stream(stream))
+
+
+def gemm_rp(prec, m, n, k, A, lda, B, ldb, C, ldc, stream=None):
+    _call("mpb_gemm_r_rp", prec, m, n, k, _ptr(A), lda, _ptr(B), ldb, _ptr(C), ldc, _stream(stream))
+
+
+def fmath_rp(name, prec, n, a, r, b=None, stream=None):
+    """elementary function `name` (FN) at a runtime precision prec, within 1 ULP of prec bits."""
+    _call("mpb_fmath_r_rp", FN.index(name), prec, n, _ptr(a), _ptr(b), _ptr(r), _stream(stream))
 
 
 def fma(prec, n, a, b, c, r, cplx=False, stream=None):

@@ -148,16 +148,19 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
+      uint32_t issued = 0u, iphase = 0u; /* per stage: a load pending on it, and its phase */
       for (long u = blockIdx.x; u < units && !abort_flag; u += gridDim.x) {
         const Unit x = decode(g, u, T);
         for (int s = x.s_lo; s <= x.s_hi && !abort_flag; ++s) {
           const int t = x.d - s;
           for (int kc = x.kc0; kc < x.kc1; ++kc) {
-            if (!sm100::mbar_wait(&empty[stage], phase ^ 1u, &abort_flag)) {
+            if (!sm100::mbar_wait(&empty[stage], phase ^ 1u, &abort_flag, g.wait_ns)) {
               fail(1);
               break;
             }
             sm100::mbar_arrive_expect_tx(&full[stage], A_STAGE + B_STAGE);
+            issued |= 1u << stage;
+            iphase = (iphase & ~(1u << stage)) | (phase << stage);
             sm100::tma_load_3d(sA + stage * A_STAGE, &tmA, kc * BK, x.ti * BM, x.q * g.S + s, &full[stage]);
             sm100::tma_load_3d(sB + stage * B_STAGE, &tmB, kc * BK, x.tj * BN, x.q * g.S + t, &full[stage]);
             if (++stage == STAGES) {
@@ -169,11 +172,18 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       }
       /* drain: wait until every issued stage has been consumed (bounded) */
       for (int q = 0; q < STAGES && !abort_flag; ++q) {
-        if (!sm100::mbar_wait(&empty[stage], phase ^ 1u, &abort_flag)) break;
+        if (!sm100::mbar_wait(&empty[stage], phase ^ 1u, &abort_flag, g.wait_ns)) break;
         if (++stage == STAGES) {
           stage = 0;
           phase ^= 1u;
         }
+      }
+      if (abort_flag) {
+        /* the consumer is gone: wait (bounded) for this CTA's own copies still
+         * in flight, so none lands in shared memory after the CTA exits */
+        volatile int never = 0;
+        for (int s2 = 0; s2 < STAGES; ++s2)
+          if ((issued >> s2) & 1u) sm100::mbar_wait(&full[s2], (iphase >> s2) & 1u, &never, g.wait_ns);
       }
     }
   } else if (warp == 1) {
@@ -186,7 +196,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       uint32_t aphase = 0;
       for (long u = blockIdx.x; u < units && !abort_flag; u += gridDim.x) {
         const Unit x = decode(g, u, T);
-        if (!sm100::mbar_wait(&tempty[acc], aphase ^ 1u, &abort_flag)) {
+        if (!sm100::mbar_wait(&tempty[acc], aphase ^ 1u, &abort_flag, g.wait_ns)) {
           fail(2);
           break;
         }
@@ -196,7 +206,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         bool ok = true;
         for (int s = x.s_lo; s <= x.s_hi && ok; ++s) {
           for (int kc = x.kc0; kc < x.kc1; ++kc) {
-            if (!sm100::mbar_wait(&full[stage], phase, &abort_flag)) {
+            if (!sm100::mbar_wait(&full[stage], phase, &abort_flag, g.wait_ns)) {
               fail(3);
               ok = false;
               break;
@@ -218,7 +228,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
           }
         }
         if (!ok) break;
-        sm100::mma_commit(&tfull[acc]);
+        if (!(g.inject == 1 && blockIdx.x == 0 && u == 0)) sm100::mma_commit(&tfull[acc]);
         if (++acc == 2) {
           acc = 0;
           aphase ^= 1u;
@@ -227,7 +237,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       /* tensor memory is freed below: wait (bounded) for every MMA issued */
       sm100::mma_commit(done);
       volatile int never = 0;
-      sm100::mbar_wait(done, 0, &never);
+      sm100::mbar_wait(done, 0, &never, g.wait_ns);
     }
   } else {
     /* ---------------- epilogue: TMEM -> int32 diagonal planes ---------------- */
@@ -237,7 +247,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     for (long u = blockIdx.x; u < units; u += gridDim.x) {
       /* tcgen05.ld is warp-collective: lane 0 waits and decides for the warp */
       int ok = 1;
-      if (lane == 0) ok = (!abort_flag && sm100::mbar_wait(&tfull[acc], aphase, &abort_flag)) ? 1 : 0;
+      if (lane == 0) ok = (!abort_flag && sm100::mbar_wait(&tfull[acc], aphase, &abort_flag, g.wait_ns)) ? 1 : 0;
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) {
         if (lane == 0) fail(4);
@@ -314,6 +324,10 @@ static bool make_tmap(CUtensorMap *tm, void *base, int kp, int rows, int planes,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+/* failure-path test: consumed by the next tensor-core launch of the process */
+static std::atomic<int> g_inject{0};
+static std::atomic<long long> g_inject_wait_ns{0};
+
 int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *err, int dl, int dh,
                      const int *tiles, const int *ntiles, cudaStream_t st) {
   CUtensorMap tmA, tmB;
@@ -339,6 +353,9 @@ int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *e
   ga.ntiles = ntiles;
   ga.D = D;
   ga.err = err;
+  ga.inject = g_inject.exchange(0);
+  const long long wns = g_inject_wait_ns.exchange(0);
+  ga.wait_ns = (ga.inject && wns > 0) ? (uint64_t)wns : sm100::kWaitNs;
   const long grid = std::min<long>(ga.units, (long)sm_count());
   const int phase = tiles ? kPhaseTensorLow : kPhaseTensor;
   profile_mark(phase, true, st);
@@ -484,5 +501,17 @@ extern "C" int mpb_gemm_exact_r_static(int prec, size_t m, size_t n, size_t k, c
     return exact::run_exact_n<N>(p, (const uint8_t *)A, lda, (const uint8_t *)B, ldb, (uint8_t *)C, ldc, ws, status,
                                  st);
   });
+  return MPB_OK;
+}
+
+/* failure-path test of the tensor-core kernel: the next launch runs with one
+ * accumulator commit withheld in its first CTA and every mbarrier wait limited
+ * to wait_ns, so that CTA's epilogue wait runs out, it raises its abort flag,
+ * records the error in status[1], waits for its own MMAs and copies, frees its
+ * tensor memory and returns */
+extern "C" int mpb_gemm_exact_test_inject(int what, long long wait_ns) {
+  if (what != 1 || wait_ns < 1000 || wait_ns > (long long)mpb::sm100::kWaitNs) return MPB_ERR_ARG;
+  mpb::exact::g_inject_wait_ns.store(wait_ns);
+  mpb::exact::g_inject.store(what);
   return MPB_OK;
 }

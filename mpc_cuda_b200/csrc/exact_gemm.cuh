@@ -386,6 +386,9 @@ struct GemmArgs {
   const int *ntiles;   /* ... *ntiles of them, counted on the device */
   int32_t *D;          /* [nprod][P][2S-1][dplane], each plane m x n */
   int *err;
+  uint64_t wait_ns;    /* limit of every mbarrier wait (sm100::kWaitNs unless a test shortens it) */
+  int inject;          /* test of the failure path: 1 = CTA 0 withholds its first accumulator
+                        * commit, so its epilogue's wait runs out; 0 otherwise */
 };
 
 /* tensor-core phase (exact_gemm.cu): TMA maps over the digit planes and the

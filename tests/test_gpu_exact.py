@@ -307,3 +307,23 @@ def test_plain_complex_pb256_full_size(orc, mpb):
         exp = orc.gemm(prec, m, n, k, A, k, B, n, cplx=True, impl="mp", rows=(r0, r1))
         bad, first = orc.mismatches(prec, got[sel], exp[sel], True)
         assert bad == 0, f"rows {r0}-{r1}: {bad} entries differ from MPC (first {first})"
+
+
+def test_tensor_kernel_wait_runs_out_and_reports(orc, mpb):
+    """The bounded-wait path of the tensor-core kernel: one launch runs with an
+    accumulator commit withheld in its first CTA and 50 ms wait limits, so that
+    CTA's epilogue wait runs out (nothing else sets the barrier).  The kernel
+    must report an error code in status[1] instead of hanging or faulting,
+    and the next call on the same stream must be correct again."""
+    L = mpb.lib()
+    assert L.mpb_gemm_exact_test_inject(2, 50_000_000) == -7  # MPB_ERR_ARG: no such injection
+    assert L.mpb_gemm_exact_test_inject(1, 10) == -7  # limit out of range
+    prec, m, n, k = 512, 256, 512, 64
+    A = rand_aos(prec, m * k, 301)
+    B = rand_aos(prec, k * n, 302)
+    assert L.mpb_gemm_exact_test_inject(1, 50_000_000) == 0
+    _, st = run_exact(mpb, prec, m, n, k, A, B, sp_bits=16)
+    assert st[1] in (1, 2, 3, 4), f"status {st}: the withheld commit was not reported"
+    C, st = run_exact(mpb, prec, m, n, k, A, B, sp_bits=16)
+    assert st.tolist() == [0, 0]
+    assert orc.mismatches(prec, C, orc.gemm_exact(prec, m, n, k, A, k, B, n, impl="mp"))[0] == 0
