@@ -1115,6 +1115,61 @@ def run_gpu(args):
     return 0
 
 
+# ------------------------------------------------------------------ kernel tour (profiling)
+def run_kernel_tour(args):
+    """One launch of each kernel family that has no workload of its own, at
+    moderate sizes, for ncu captures (`ncu -k regex:... python bench.py
+    --workload kernel_tour`): GEMV at 512 bits (one thread per row) and at 2048
+    bits (cooperative), the plain complex GEMM at 256 bits (256^3), the exact
+    GEMM's preparation and tail stages (512^3 at 512 bits), division and square
+    root (2^18 at 512 bits), sine and complex exponential (2^16 at 512 bits) and
+    the cooperative complex AXPY (2^16 at 1024 bits).  Prints one JSON line
+    with the wall time of the tour; not a throughput measurement."""
+    import torch
+
+    import mpc_cuda_b200 as M
+    from mpc_cuda_b200 import layout, synth
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(3)
+
+    def vec(prec, n, e=8, cplx=False):
+        if cplx:
+            re, im = synth.random_elems(rng, prec, n, -e, e), synth.random_elems(rng, prec, n, -e, e)
+            return torch.from_numpy(layout.aos_to_vec(prec, synth.interleave_complex(prec, re, im), True).copy()).cuda()
+        lm, hd = synth.random_elems(rng, prec, n, -e, e)
+        return torch.from_numpy(layout.vec_from_parts(prec, lm, hd).copy()).cuda()
+
+    def posvec(prec, n):
+        lm, hd = synth.random_elems(rng, prec, n, -8, 8)
+        return torch.from_numpy(layout.vec_from_parts(prec, lm, hd & ~np.uint32(1)).copy()).cuda()
+
+    t0 = time.time()
+    m, n = 4096, 256
+    M.gemv(512, m, n, vec(512, m * n), n, vec(512, n), vec(512, m), M.empty(512, m))
+    m, n = 512, 256
+    M.gemv(2048, m, n, vec(2048, m * n), n, vec(2048, n), vec(2048, m), M.empty(2048, m))
+    m = 256
+    M.gemm(256, m, m, m, vec(256, m * m, cplx=True), m, vec(256, m * m, cplx=True), m, M.empty(256, m * m, True), m,
+           cplx=True)
+    m = 512
+    M.gemm_exact(512, m, m, m, vec(512, m * m), m, vec(512, m * m), m, M.empty(512, m * m), m, sp_bits=32)
+    n = 1 << 18
+    M.div(512, n, vec(512, n), vec(512, n), M.empty(512, n))
+    M.sqrt(512, n, posvec(512, n), M.empty(512, n))
+    n = 1 << 16
+    M.fmath("sin", 512, n, vec(512, n, e=2), M.empty(512, n))
+    M.cfmath("exp", 512, n, vec(512, n, e=2, cplx=True), M.empty(512, n, True))
+    old = M.get_split(M.SPLIT_AXPY_C, 1024)
+    M.set_split(M.SPLIT_AXPY_C, 1024, 4)
+    M.axpy(1024, n, vec(1024, 1, cplx=True), vec(1024, n, cplx=True), vec(1024, n, cplx=True),
+           M.empty(1024, n, True), cplx=True)
+    M.set_split(M.SPLIT_AXPY_C, 1024, old)
+    torch.cuda.synchronize()
+    print(json.dumps({"workload": "kernel_tour", "wall_s": round(time.time() - t0, 3), "note": "profiling aid"}))
+    return 0
+
+
 # ------------------------------------------------------------------ drop-in user kernels
 DROPIN_PRECS = (64, 96, 128, 160, 256, 288, 512, 1024, 1056, 2048)
 
@@ -1241,7 +1296,7 @@ def main():
                     help="timed steps (default: the workload's, about 2 s of GPU time)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("mpb", "reference"), default="mpb")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["dropin_axpy"], default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["dropin_axpy", "kernel_tour"], default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--split", type=int, default=0,
@@ -1258,6 +1313,8 @@ def main():
         args.warmup = 3
     if args.workload == "dropin_axpy":
         return run_dropin(args)
+    if args.workload == "kernel_tour":
+        return run_kernel_tour(args)
     if args.steps is None:
         args.steps = WORKLOADS[args.workload]().default_steps
     if args.impl == "reference":

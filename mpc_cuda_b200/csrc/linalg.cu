@@ -149,12 +149,18 @@ static int bufs_ok(std::initializer_list<const void *> bufs) {
 
 using namespace mpb;
 
+/* GEMV blocks: one warp each when the rows give fewer than four warps per SM
+ * (a tall matrix of wide operands is few warps: 4096 rows of one thread each
+ * are 32 blocks of 128 on 148 SMs), four warps otherwise */
+static int gemv_block(size_t warps) { return warps < 4u * (size_t)sm_count() ? 32 : kGemvBlock; }
+
 template <int L, int G>
 static void launch_gemv_coop_lg(size_t m, size_t n, const uint8_t *A, size_t lda, const uint8_t *x, const uint8_t *y,
                                 uint8_t *yo, cudaStream_t st) {
   const size_t warps = (m + 32 / G - 1) / (32 / G);
-  const int g = grid_for(k_gemv_r_coop<L, G>, kGemvBlock, warps * 32u);
-  k_gemv_r_coop<L, G><<<g, kGemvBlock, 0, st>>>(m, n, A, lda, x, y, yo);
+  const int b = gemv_block(warps);
+  const int g = grid_for(k_gemv_r_coop<L, G>, b, warps * 32u);
+  k_gemv_r_coop<L, G><<<g, b, 0, st>>>(m, n, A, lda, x, y, yo);
 }
 /* the cooperative GEMV at N limbs with `lanes` lanes per row (1024 bits: 4 or
  * 8 lanes, 2048 bits: 8 or 16; mpb_set_split validates) */
@@ -193,17 +199,18 @@ static int gemv_entry(int prec, size_t m, size_t n, const void *A, size_t lda, c
   rc = bufs_ok({A, x, y, yo});
   if (rc != MPB_OK) return rc;
   MPB_DISPATCH_PREC(prec, {
+    const int b = gemv_block(tiles_for(m));
     if (CPLX) {
-      const int g = grid_for(k_gemv_c<N>, kGemvBlock, tiles_for(m) * 32u);
-      k_gemv_c<N><<<g, kGemvBlock, 0, as_stream(stream)>>>(m, n, (const uint8_t *)A, lda, (const uint8_t *)x,
-                                                            (const uint8_t *)y, (uint8_t *)yo);
+      const int g = grid_for(k_gemv_c<N>, b, tiles_for(m) * 32u);
+      k_gemv_c<N><<<g, b, 0, as_stream(stream)>>>(m, n, (const uint8_t *)A, lda, (const uint8_t *)x,
+                                                   (const uint8_t *)y, (uint8_t *)yo);
     } else if (N >= 32 && split_lanes(MPB_SPLIT_GEMV_R, prec) > 1) {
       launch_gemv_coop<N>(split_lanes(MPB_SPLIT_GEMV_R, prec), m, n, (const uint8_t *)A, lda, (const uint8_t *)x,
                           (const uint8_t *)y, (uint8_t *)yo, as_stream(stream));
     } else {
-      const int g = grid_for(k_gemv_r<N>, kGemvBlock, tiles_for(m) * 32u);
-      k_gemv_r<N><<<g, kGemvBlock, 0, as_stream(stream)>>>(m, n, (const uint8_t *)A, lda, (const uint8_t *)x,
-                                                            (const uint8_t *)y, (uint8_t *)yo);
+      const int g = grid_for(k_gemv_r<N>, b, tiles_for(m) * 32u);
+      k_gemv_r<N><<<g, b, 0, as_stream(stream)>>>(m, n, (const uint8_t *)A, lda, (const uint8_t *)x,
+                                                   (const uint8_t *)y, (uint8_t *)yo);
     }
   });
   return launch_status();
