@@ -457,20 +457,24 @@ MPB_HD bool add_round(fval<NM> &r, const uint32_t *xm, int32_t xe, uint32_t xs,
   const uint32_t q = (d >> 5) < (uint32_t)W ? (d >> 5) : (uint32_t)W;
   const uint32_t rs = d & 31u;
   uint32_t st = 0u;
-  MPB_UNROLL
-  for (int k = 0; k < KQ; ++k) {
-    constexpr int dummy = 0;
-    (void)dummy;
-    const int sh = 1 << k;
-    const bool on = (q >> k) & 1u;
-    uint32_t lost = 0u;
+  /* whole-word part of the shift: a log-depth select network, skipped when no
+   * lane of the warp shifts by a word or more (exponents within 32 bits, the
+   * common case of AXPY and dot-product operands; the network is the identity
+   * for q = 0) */
+  if (any_lane<kVote>(q != 0u)) {
     MPB_UNROLL
-    for (int i = 0; i < sh && i < W; ++i) lost |= Y[i];
-    st |= on ? lost : 0u;
-    MPB_UNROLL
-    for (int i = 0; i < W; ++i) {
-      const uint32_t src = (i + sh < W) ? Y[i + sh] : 0u;
-      Y[i] = on ? src : Y[i];
+    for (int k = 0; k < KQ; ++k) {
+      const int sh = 1 << k;
+      const bool on = (q >> k) & 1u;
+      uint32_t lost = 0u;
+      MPB_UNROLL
+      for (int i = 0; i < sh && i < W; ++i) lost |= Y[i];
+      st |= on ? lost : 0u;
+      MPB_UNROLL
+      for (int i = 0; i < W; ++i) {
+        const uint32_t src = (i + sh < W) ? Y[i + sh] : 0u;
+        Y[i] = on ? src : Y[i];
+      }
     }
   }
   st |= Y[0] & ((1u << rs) - 1u);
