@@ -457,13 +457,15 @@ MPB_HD bool add_round(fval<NM> &r, const uint32_t *xm, int32_t xe, uint32_t xs,
   const uint32_t q = (d >> 5) < (uint32_t)W ? (d >> 5) : (uint32_t)W;
   const uint32_t rs = d & 31u;
   uint32_t st = 0u;
-  /* whole-word part of the shift: a log-depth select network, skipped when no
-   * lane of the warp shifts by a word or more (exponents within 32 bits, the
-   * common case of AXPY and dot-product operands; the network is the identity
-   * for q = 0) */
-  if (any_lane<kVote>(q != 0u)) {
+  /* whole-word part of the shift: a log-depth select network.  Only as many
+   * stages run as the warp needs: none when no lane shifts by a word or more
+   * (exponents within 32 bits), two when every lane shifts by at most 3 words
+   * (the common case of AXPY and dot-product operands), else all KQ. */
+  const int kq_run = any_lane<kVote>(q >= 4u) ? KQ : (any_lane<kVote>(q != 0u) ? 2 : 0);
+  if (kq_run != 0) {
     MPB_UNROLL
     for (int k = 0; k < KQ; ++k) {
+      if (k >= 2 && kq_run == 2) break;
       const int sh = 1 << k;
       const bool on = (q >> k) & 1u;
       uint32_t lost = 0u;
@@ -511,12 +513,17 @@ MPB_HD bool add_round(fval<NM> &r, const uint32_t *xm, int32_t xe, uint32_t xs,
   for (int i = 0; i < W; ++i) D[i] = fshr(D[i], D[i + 1], cs);
 
   /* ---- normalise left (cancellation after subtraction) ---- */
-  uint32_t lq = (uint32_t)W, top = 0u;
-  MPB_UNROLL
-  for (int i = W - 1; i >= 0; --i) {
-    const bool take = (lq == (uint32_t)W) && (D[i] != 0u);
-    top = take ? D[i] : top;
-    lq = take ? (uint32_t)(W - 1 - i) : lq;
+  /* the leading word is the top one unless a subtraction cancelled 32 bits or
+   * more: search the window only when some lane needs it */
+  uint32_t lq = 0u, top = D[W - 1];
+  if (any_lane<kVote>(top == 0u)) {
+    lq = (uint32_t)W;
+    MPB_UNROLL
+    for (int i = W - 1; i >= 0; --i) {
+      const bool take = (lq == (uint32_t)W) && (D[i] != 0u);
+      top = take ? D[i] : top;
+      lq = take ? (uint32_t)(W - 1 - i) : lq;
+    }
   }
   const bool zero = (lq == (uint32_t)W);
   const uint32_t lr = clz32(top) & 31u;
@@ -557,7 +564,7 @@ MPB_HD bool add_round(fval<NM> &r, const uint32_t *xm, int32_t xe, uint32_t xs,
   rndn<NM, kRnd>(r.m, e, g >> 31, st);
   r.e = e;
   r.s = s;
-  if (zero) set_zero(r);
+  if (any_lane<kVote>(zero) && zero) set_zero(r); /* x = -y exactly */
   return ok;
 }
 
