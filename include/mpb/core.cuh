@@ -392,6 +392,46 @@ MPB_HD void mul(fval<N> &r, const fval<N> &a, const fval<N> &b) {
   mul_limbs<N, kRnd>(r, a, b.m, b.e, b.s);
 }
 
+/* r = round(a * b) for a b whose limbs below the top K are zero (a scalar
+ * converted from a double has K <= 2, a small integer K = 1): the exact
+ * N x K product (N+K words, N*K partial products in the column order of
+ * mul_full) lands in the top of the 2N-word array and is rounded once, so no
+ * certification is needed. */
+template <int N, int K>
+MPB_HD void mul_short(fval<N> &r, const fval<N> &a, const uint32_t *bm, int32_t be, uint32_t bs) {
+  static_assert(K >= 1 && K < N, "short operand");
+  uint32_t p[2 * N];
+  MPB_UNROLL
+  for (int i = 0; i < N - K; ++i) p[i] = 0u;
+  uint32_t c0 = 0u, c1 = 0u, c2 = 0u;
+  MPB_UNROLL
+  for (int c = 0; c < N + K - 1; ++c) {
+    MPB_UNROLL
+    for (int j = 0; j < K; ++j) {
+      const int i = c - j;
+      if (i < 0 || i >= N) continue;
+      uint32_t cf = 0;
+      c0 = madlo_cc(a.m[i], bm[N - K + j], c0, cf);
+      c1 = madchi_cc(a.m[i], bm[N - K + j], c1, cf);
+      c2 = addc(c2, 0u, cf);
+    }
+    p[N - K + c] = c0;
+    c0 = c1;
+    c1 = c2;
+    c2 = 0u;
+  }
+  p[2 * N - 1] = c0;
+  round_prod<N>(r, p, a.e + be, a.s ^ bs);
+  if (is_zero(a) || be == kExpZero) set_zero(r);
+}
+/* the number of limbs of b from the top down to its lowest nonzero limb (1 for zero) */
+template <int N>
+MPB_HD int limb_length(const uint32_t *bm) {
+  int k = N;
+  while (k > 1 && bm[N - k] == 0u) --k;
+  return k;
+}
+
 /* exact product, normalised so that bit 31 of p[2N-1] is set (zero stays 0) */
 template <int N>
 MPB_HD void mul_exact_norm(uint32_t *p, int32_t &e, const fval<N> &a, const fval<N> &b) {

@@ -198,23 +198,39 @@ __global__ void __launch_bounds__(kBlock) k_binop_c(size_t n, int op, const uint
 /* ---- AXPY ---- */
 /* z = round(round(a*x) + y): the scalar a lives in shared memory (warp-
  * uniform broadcast reads, no registers held), and it is the row multiplier
- * of the schoolbook product, so each of its limbs is read once per product. */
+ * of the schoolbook product, so each of its limbs is read once per product.
+ * A scalar whose limbs below the top one or two are zero (one converted from
+ * a double, a small integer: 1.5, 2, -0.25 ...) takes the exact short product
+ * (mul_short: N or 2N partial products instead of the ~N^2/2 upper columns);
+ * the branch is uniform over the grid and the result is the same. */
 template <int N>
 __global__ void __launch_bounds__(kBlock) k_axpy_r(size_t n, const uint8_t *a, const uint8_t *x, const uint8_t *y,
                                                    uint8_t *z) {
   __shared__ fval<N> sa;
+  __shared__ int klen;
   if (threadIdx.x == 0) {
     fval<N> t;
     load_elem<N>(t, a, 0);
     sa = t;
+    klen = limb_length<N>(t.m);
   }
   __syncthreads();
+  const int kl = N > 2 ? klen : N;
   const size_t np = tiles_for(n) * 32u;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
     fval<N> xv, yv, t, r;
     load_elem<N, kStream>(xv, x, i);
-    mul<N>(t, xv, sa);
     load_elem<N, kStream>(yv, y, i);
+    if constexpr (N > 2) {
+      if (kl == 1)
+        mul_short<N, 1>(t, xv, sa.m, sa.e, sa.s);
+      else if (kl == 2)
+        mul_short<N, 2>(t, xv, sa.m, sa.e, sa.s);
+      else
+        mul<N>(t, xv, sa);
+    } else {
+      mul<N>(t, xv, sa);
+    }
     add<N, true>(r, t, yv);
     if (i < n) store_elem<N, kStream>(z, i, r);
   }

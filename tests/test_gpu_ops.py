@@ -228,6 +228,22 @@ def test_axpy_real_pb256_full_size(orc, mpb):
     assert bad == 0, f"first mismatch {first}"
 
 
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("scalar", (1.5, 3.0, -0.1, 2.0 ** -700, 1e300, -7.0 / 3.0, 0.0))
+def test_axpy_short_scalar(orc, mpb, prec, scalar):
+    """Scalars with one or two nonzero limbs (small integers, doubles) take the
+    exact short product in the real AXPY; x and y are full random operands.
+    With a = 1.5 or 3 a quarter of the products drop exactly half an ULP, so
+    the ties-to-even path is exercised too."""
+    n = 20000 if prec <= 1024 else 4000
+    X, Y = orc.gen_pairs(prec, n, 0xA5 + prec)
+    a = orc.from_double(prec, [scalar])
+    z = mpb.empty(prec, n)
+    mpb.axpy(prec, n, dvec(prec, a), dvec(prec, X), dvec(prec, Y), z)
+    bad, first = orc.mismatches(prec, hvec(prec, z, n), orc.axpy(prec, a, X, Y, impl="mp"))
+    assert bad == 0, f"axpy PB={prec} a={scalar}: first mismatch {first}"
+
+
 def test_axpy_complex_pb1024_full_size(orc, mpb):
     """The complex AXPY workload at full size (PB=1024, n=2^18, 1% zeros)."""
     prec, n = 1024, 1 << 18
