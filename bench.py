@@ -392,8 +392,13 @@ class GemmWorkload:
         """plain kernel rate on the same operands, dominant-kernel time, status"""
         import torch
 
+        from mpc_cuda_b200 import tune
+
         M = self.M
         c = self.cplx
+        # the plain kernel's block shape, tuned for this C on a short k
+        tune.autotune_gemm_warps(self.prec, self.m, self.n, min(self.k, 64), c)
+        warps = M.get_gemm_warps(self.prec, c)
         M.gemm(self.prec, self.m, self.n, self.k, self.dA, self.k, self.dB, self.n, self.dC2, self.n, c, stream=stream)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -406,7 +411,7 @@ class GemmWorkload:
         plain_ms = e0.elapsed_time(e1) / steps
         st = self.status.cpu().tolist()
         return {"plain_ms_per_step": plain_ms, "plain_value": self.units() / (plain_ms / 1e3), "status": st,
-                "accuracy": self.accuracy()}
+                "plain_warps": warps, "accuracy": self.accuracy()}
 
     def accuracy(self, rows=(0, None, -1)):
         """Error of the timed exact GEMM's result on a row sample (first, middle
@@ -1103,7 +1108,8 @@ def run_gpu(args):
         if extra:
             line["plain"] = {"value": extra["plain_value"], "unit": "mp-FMA/s",
                              "ms_per_step": extra["plain_ms_per_step"],
-                             "kernel": "k_gemm_r (sequential-k, per-operation rounding)"}
+                             "kernel": "k_gemm_r (sequential-k, per-operation rounding)",
+                             "warps_per_block": extra.get("plain_warps")}
             line["exact_over_plain"] = line["value"] / extra["plain_value"]
             line["status"] = {"fallback_rows_cols": extra["status"][0], "kernel_error": extra["status"][1]}
             if extra.get("accuracy"):

@@ -238,6 +238,18 @@ enum { MPB_SPLIT_AXPY_C = 0, MPB_SPLIT_GEMV_R = 1 };
 int mpb_set_split(int kind, int prec, int lanes);
 int mpb_get_split(int kind, int prec, int *lanes);
 
+/* ---- plain GEMM block shape ---- */
+/* The plain GEMM (mpb_gemm_r / mpb_gemm_c) runs one thread per output: a warp
+ * owns one row of C and 32 columns, a block `warps` rows (4, 8 or 16).  Few
+ * blocks (a small C) favour 4, wide operands whose register need caps the
+ * resident blocks may favour 16; results are identical for every shape.  The
+ * setting is process-wide per real/complex and precision, read at every
+ * launch (default 8); mpc_cuda_b200.tune.autotune_gemm_warps times the shapes
+ * on a problem and keeps the fastest.  Returns MPB_ERR_ARG for another
+ * warp count. */
+int mpb_set_gemm_warps(int cplx, int prec, int warps);
+int mpb_get_gemm_warps(int cplx, int prec, int *warps);
+
 /* ---- batched GEMV: thousands of independent problems, mixed sizes and precisions ---- */
 /* One problem y_out = A.x + y (real, prec bits, same order as mpb_gemv_r).
  * Device pointers; lda a multiple of 32 (>= n); m or n may be 0. */

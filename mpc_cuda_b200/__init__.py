@@ -92,6 +92,8 @@ _SIGS = {
     "mpb_batch_gemv_set_split": ([_V, _I, _I], C.c_int),
     "mpb_set_split": ([_I, _I, _I], C.c_int),
     "mpb_get_split": ([_I, _I, C.POINTER(_I)], C.c_int),
+    "mpb_set_gemm_warps": ([_I, _I, _I], C.c_int),
+    "mpb_get_gemm_warps": ([_I, _I, C.POINTER(_I)], C.c_int),
     "mpb_batch_gemv_destroy": ([_V], None),
     "mpb_gemm_exact_workspace": ([_I, _S, _S, _S, _I], C.c_size_t),
     "mpb_profile_enable": ([_I], None),
@@ -380,6 +382,17 @@ def set_split(kind, prec, lanes):
 def get_split(kind, prec):
     v = C.c_int()
     _call("mpb_get_split", int(kind), int(prec), C.byref(v))
+    return v.value
+
+
+def set_gemm_warps(prec, warps, cplx=False):
+    """Warps (rows of C) per block of the plain GEMM at `prec`: 4, 8 or 16."""
+    _call("mpb_set_gemm_warps", 1 if cplx else 0, int(prec), int(warps))
+
+
+def get_gemm_warps(prec, cplx=False):
+    v = C.c_int()
+    _call("mpb_get_gemm_warps", 1 if cplx else 0, int(prec), C.byref(v))
     return v.value
 
 

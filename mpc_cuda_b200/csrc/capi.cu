@@ -95,6 +95,18 @@ int split_lanes(int kind, int prec) {
   return g_split[kind][g].load(std::memory_order_relaxed);
 }
 
+/* ---------------- plain GEMM block shape ---------------- */
+static std::atomic<int> g_gemm_warps[2][6] = {{{kDefaultGemmWarps}, {kDefaultGemmWarps}, {kDefaultGemmWarps},
+                                               {kDefaultGemmWarps}, {kDefaultGemmWarps}, {kDefaultGemmWarps}},
+                                              {{kDefaultGemmWarps}, {kDefaultGemmWarps}, {kDefaultGemmWarps},
+                                               {kDefaultGemmWarps}, {kDefaultGemmWarps}, {kDefaultGemmWarps}}};
+
+int gemm_warps(int cplx, int prec) {
+  const int g = prec_group(prec);
+  if (g < 0) return kDefaultGemmWarps;
+  return g_gemm_warps[cplx ? 1 : 0][g].load(std::memory_order_relaxed);
+}
+
 } /* namespace mpb */
 
 extern "C" int mpb_set_split(int kind, int prec, int lanes) {
@@ -113,6 +125,22 @@ extern "C" int mpb_get_split(int kind, int prec, int *lanes) {
   if (kind < 0 || kind >= kSplitKinds) return MPB_ERR_ARG;
   if (prec_group(prec) < 0) return MPB_ERR_PREC;
   *lanes = split_lanes(kind, prec);
+  return MPB_OK;
+}
+
+extern "C" int mpb_set_gemm_warps(int cplx, int prec, int warps) {
+  using namespace mpb;
+  if (prec_group(prec) < 0) return MPB_ERR_PREC;
+  if (warps != 4 && warps != 8 && warps != 16) return MPB_ERR_ARG;
+  g_gemm_warps[cplx ? 1 : 0][prec_group(prec)].store(warps, std::memory_order_relaxed);
+  return MPB_OK;
+}
+
+extern "C" int mpb_get_gemm_warps(int cplx, int prec, int *warps) {
+  using namespace mpb;
+  if (!warps) return MPB_ERR_NULL;
+  if (prec_group(prec) < 0) return MPB_ERR_PREC;
+  *warps = gemm_warps(cplx, prec);
   return MPB_OK;
 }
 

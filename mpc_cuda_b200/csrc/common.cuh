@@ -75,6 +75,10 @@ constexpr int kDefaultSplitAxpyC1024 = 1; /* complex AXPY elements at 1024 bits 
 int split_lanes(int kind, int prec);
 bool split_supported(int kind, int prec, int lanes);
 
+/* plain GEMM warps per block (mpb_set_gemm_warps): 4, 8 or 16 */
+constexpr int kDefaultGemmWarps = 8;
+int gemm_warps(int cplx, int prec);
+
 /* Opt-in phase timing (mpb_profile_enable): entry points that run several
  * kernels record a CUDA event pair around each phase on the caller's stream. */
 enum {

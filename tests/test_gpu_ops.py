@@ -257,6 +257,29 @@ def test_axpy_complex_pb1024_full_size(orc, mpb):
 
 @pytest.mark.parametrize("cplx", (False, True))
 @pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("warps", (4, 16))
+def test_gemm_plain_block_shapes(orc, mpb, prec, warps, cplx):
+    """every block shape of the plain GEMM (mpb_set_gemm_warps) gives the MPFR/MPC result"""
+    m, n, k = (37, 70, 19) if prec <= 1024 else (9, 33, 7)
+    A, _ = orc.gen_pairs(prec, m * k, 0x63 + warps + prec, cplx)
+    B, _ = orc.gen_pairs(prec, k * n, 0x64 + warps + prec, cplx)
+    lda, ldb, ldc = (-(-k // 32) * 32, -(-n // 32) * 32, -(-n // 32) * 32)
+    Cd = mpb.empty(prec, m * ldc, cplx)
+    old = mpb.get_gemm_warps(prec, cplx)
+    try:
+        mpb.set_gemm_warps(prec, warps, cplx)
+        mpb.gemm(prec, m, n, k, dvec(prec, pad_rows(prec, A, m, k, lda, cplx), cplx), lda,
+                 dvec(prec, pad_rows(prec, B, k, n, ldb, cplx), cplx), ldb, Cd, ldc, cplx)
+    finally:
+        mpb.set_gemm_warps(prec, old, cplx)
+    got = unpad_rows(hvec(prec, Cd, m * ldc, cplx), m, n, ldc)
+    exp = orc.gemm(prec, m, n, k, A, k, B, n, cplx, impl="mp")
+    bad, first = orc.mismatches(prec, got, exp, cplx)
+    assert bad == 0, f"gemm PB={prec} warps={warps}: first mismatch {first}"
+
+
+@pytest.mark.parametrize("cplx", (False, True))
+@pytest.mark.parametrize("prec", PRECS)
 @pytest.mark.parametrize("shape", ((1, 1, 1), (5, 7, 33), (33, 40, 17), (64, 64, 64)))
 def test_gemm_plain(orc, mpb, prec, shape, cplx):
     m, n, k = shape

@@ -71,3 +71,42 @@ def test_batch_tuning_reinstalls_from_cache(mpb, tmp_path):
     assert b2.tuning() == b.tuning() and b2.splits() == b.splits()
     b.close()
     b2.close()
+
+
+def test_gemm_warps_setting_and_cache(mpb, tmp_path):
+    old = mpb.get_gemm_warps(512)
+    try:
+        mpb.set_gemm_warps(512, 4)
+        assert mpb.get_gemm_warps(512) == 4
+        assert mpb.get_gemm_warps(512, cplx=True) == 8  # real and complex are separate
+        with pytest.raises(mpb.MpbError):
+            mpb.set_gemm_warps(512, 6)
+        with pytest.raises(mpb.MpbError):
+            mpb.set_gemm_warps(300, 8)
+        c = tune.TuningCache(os.path.join(tmp_path, "g.json"))
+        c.record_gemm_warps(512, 128, 128, 16)
+        c.record_gemm_warps(256, 512, 512, 4, cplx=True)
+        with pytest.raises(ValueError):
+            c.record_gemm_warps(512, 128, 128, 32)
+        c.save()
+        c2 = tune.TuningCache(c.path)
+        assert c2.apply_gemm_warps(512, 120, 100) == 16
+        assert mpb.get_gemm_warps(512) == 16
+        assert c2.lookup_gemm_warps(256, 512, 512, cplx=True) == 4
+        assert c2.lookup_gemm_warps(256, 512, 512) is None
+    finally:
+        mpb.set_gemm_warps(512, old)
+
+
+@pytest.mark.gpu
+def test_autotune_gemm_warps_picks_the_fastest(mpb, tmp_path):
+    c = tune.TuningCache(os.path.join(tmp_path, "t.json"))
+    old = mpb.get_gemm_warps(512)
+    try:
+        times = tune.autotune_gemm_warps(512, 128, 128, 64, cache=c)
+        assert set(times) == {4, 8, 16}
+        best = min(times, key=times.get)
+        assert mpb.get_gemm_warps(512) == best
+        assert c.lookup_gemm_warps(512, 128, 128) == best
+    finally:
+        mpb.set_gemm_warps(512, old)
