@@ -682,7 +682,9 @@ MPB_HD void mul_high_norm(uint32_t *p, int32_t &e, const fval<N> &a, const fval<
  * i.e. below 2^(e_i - 32N - 25) for |product| < 2^(e_i), so the sum is off by
  * less than 2^(e_max - 32N - 24).  add_round certifies the rounding against
  * that (it fails under heavy cancellation -- more than about 20 bits -- or
- * next to a midpoint), and the exact products decide otherwise. */
+ * next to a midpoint), and the exact products decide otherwise.  The words
+ * under column N-2 of a normalised upper-column product are zero, so the sum
+ * takes the top N+2 words of each (an (N+4)-word window instead of 2N+2). */
 template <int N, bool kVote = false>
 MPB_HD void fmms(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &c,
                  const fval<N> &d, uint32_t negate_cd = 1u) {
@@ -692,7 +694,7 @@ MPB_HD void fmms(fval<N> &r, const fval<N> &a, const fval<N> &b, const fval<N> &
   if (N >= 4) {
     mul_high_norm<N>(p1, e1, a, b);
     mul_high_norm<N>(p2, e2, c, d);
-    const bool ok = add_round<2 * N, N, kVote, 32 * N + 24>(r, p1, e1, a.s ^ b.s, p2, e2, s2);
+    const bool ok = add_round<N + 2, N, kVote, 32 * N + 24>(r, p1 + (N - 2), e1, a.s ^ b.s, p2 + (N - 2), e2, s2);
     if (!ok && !(e1 == kExpZero && e2 == kExpZero)) fmms_full<N>(r, a, b, c, d, negate_cd);
   } else {
     mul_exact_norm<N>(p1, e1, a, b);
