@@ -50,7 +50,7 @@
  *
  * Work: nprod*2*m*n*k*pairs int8 operations, pairs = the slice pairs on the
  * diagonals [d0, 2S-2] (mpb_gemm_exact_plan_info; S = ceil((PB+SP+2)/8)
- * real, ceil((PB+SP+3)/8) complex; S = 69, d0 = 63, 2745 of S^2 = 4761
+ * real, ceil((PB+SP+3)/8) complex; S = 69, d0 = 65, 2616 of S^2 = 4761
  * pairs at PB=512, k=1024 with a 32-bit budget).
  * Scratch (caller-provided workspace, mpb_gemm_exact_workspace /
  * mpb_gemm_exact_c_workspace): digit planes nprod*S*(m+n)*kp bytes and the

@@ -91,9 +91,9 @@ def test_exact_gemm_workspace_and_checks(mpb):
     need = L.mpb_gemm_exact_workspace(512, m, m, m, 32)
     planes = S * 2 * m * m + 137 * (m * m + 1056) * 4 + m * m
     assert planes <= need <= planes + 64 * 1024
-    # the tensor cores skip the low diagonals 0..62: 2745 of the 69^2 slice pairs
-    assert mpb.gemm_exact_info(512, m, m, m, 32) == (69, 63, 2745)
-    assert mpb.gemm_exact_info(256, 512, 512, 512, 16, cplx=True) == (35, 27, 847)
+    # the tensor cores skip the low diagonals 0..64: 2616 of the 69^2 slice pairs
+    assert mpb.gemm_exact_info(512, m, m, m, 32) == (69, 65, 2616)
+    assert mpb.gemm_exact_info(256, 512, 512, 512, 16, cplx=True) == (35, 29, 790)
     assert L.mpb_gemm_exact_workspace(96, 8, 8, 8, 32) == 0
     good = 4096
     # missing workspace, misaligned workspace, bad leading dimension
