@@ -845,7 +845,7 @@ class CfnWorkload(AxpyWorkload):
 NCU_TRAFFIC = {
     "axpy_r256": (82.6e6, "k_axpy_r<8>, profiles/k_axpy_r_pb256_n1048576.md"),
     "axpy_c1024": (180.0e6, "k_axpy_c<32>, profiles/k_axpy_c_pb1024_n262144.md"),
-    "gemm_r512": (1.388e9, "k_diag_gemm main pass, profiles/k_diag_gemm_gemm_r512_1024cube.md"),
+    "gemm_r512": (1.314e9, "k_diag_gemm main pass, profiles/k_diag_gemm_gemm_r512_1024cube.md"),
 }
 
 WORKLOADS = {
