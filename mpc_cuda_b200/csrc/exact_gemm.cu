@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
    * previous kernel on the stream) */
   const long T = g.tiles ? (long)*g.ntiles : (long)g.mt * g.nt;
   const long units = g.tiles ? T * g.nprod * (g.dh - g.dl + 1) * g.P : g.units;
+  if (units == 0) return; /* an empty recomputation pass: no set-up at all */
   if (threadIdx.x == 0) {
     abort_flag = 0;
     for (int s = 0; s < STAGES; ++s) {

@@ -178,6 +178,8 @@ __global__ void __launch_bounds__(256) k_col_stats(int n, int k, const uint8_t *
   const int k0 = blockIdx.y * kColRows, k1 = min(k, k0 + kColRows);
   int32_t emax = kColNone, emin = kColMinNone;
   if (j < n) {
+    /* unrolled: several rows' head loads in flight per lane */
+#pragma unroll 4
     for (int kk = k0 + w; kk < k1; kk += 8) {
 #pragma unroll
       for (int part = 0; part < (CPLX ? 2 : 1); ++part) {
@@ -226,6 +228,7 @@ __global__ void __launch_bounds__(256) k_row_stats(int m, int k, const uint8_t *
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= m) return;
   int32_t emax = kExpZero, emin = 0x7fffffff;
+#pragma unroll 4
   for (int k0 = 0; k0 < k; k0 += 32) {
     const int kk = k0 + lane;
     if (kk < k) {
@@ -791,21 +794,10 @@ __global__ void __launch_bounds__(128) k_exact_round_parts(int m, int n, int S, 
   }
 }
 
-/* flagged rows / columns: plain sequential-k per-operation rounding */
+/* one entry of C by the plain per-operation kernel's order */
 template <int N, bool CPLX>
-__global__ void __launch_bounds__(256) k_fallback(size_t m, size_t n, size_t K, const uint8_t *A, size_t lda,
-                                                  const uint8_t *B, size_t ldb, uint8_t *C, size_t ldc,
-                                                  const uint8_t *rowF, const uint8_t *colF, const int *cnt,
-                                                  int *status) {
-  pdl_wait(); /* launched after the previous stage with launch_pdl */
-  if (status && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
-    status[0] = cnt[0]; /* fallback rows + columns, counted by k_row_stats */
-    status[1] = cnt[1]; /* error code of the tensor-core launches */
-  }
-  const size_t i = (size_t)blockIdx.y * 8 + (threadIdx.x >> 5);
-  const size_t j = (size_t)blockIdx.x * 32u + (threadIdx.x & 31u);
-  if (i >= m || j >= n) return;
-  if (!rowF[i] && !colF[j]) return;
+__device__ __forceinline__ void fallback_entry(size_t i, size_t j, size_t K, const uint8_t *A, size_t lda,
+                                               const uint8_t *B, size_t ldb, uint8_t *C, size_t ldc) {
   if (CPLX) {
     fval<N> cr, ci;
     set_zero(cr);
@@ -833,6 +825,28 @@ __global__ void __launch_bounds__(256) k_fallback(size_t m, size_t n, size_t K, 
   }
 }
 
+/* flagged rows / columns: plain sequential-k per-operation rounding */
+template <int N, bool CPLX>
+__global__ void __launch_bounds__(256) k_fallback(size_t m, size_t n, size_t K, const uint8_t *A, size_t lda,
+                                                  const uint8_t *B, size_t ldb, uint8_t *C, size_t ldc,
+                                                  const uint8_t *rowF, const uint8_t *colF, const int *cnt,
+                                                  int *status) {
+  pdl_wait(); /* launched after the previous stage with launch_pdl */
+  if (status && blockIdx.x == 0 && threadIdx.x == 0) {
+    status[0] = cnt[0]; /* fallback rows + columns, counted by k_row_stats */
+    status[1] = cnt[1]; /* error code of the tensor-core launches */
+  }
+  if (cnt[0] == 0) return; /* nothing flagged: the common case ends here */
+  /* blocks of 8 rows x 32 columns of C, strided over a one-wave grid */
+  const size_t tj = (n + 31) / 32, nblk = tj * ((m + 7) / 8);
+  for (size_t b = blockIdx.x; b < nblk; b += gridDim.x) {
+    const size_t i = (b / tj) * 8 + (threadIdx.x >> 5);
+    const size_t j = (b % tj) * 32u + (threadIdx.x & 31u);
+    if (i >= m || j >= n) continue;
+    if (!rowF[i] && !colF[j]) continue;
+    fallback_entry<N, CPLX>(i, j, K, A, lda, B, ldb, C, ldc);
+  }
+}
 /* the counters and column statistics every call starts from (one launch in
  * place of four memsets, so the whole chain is kernel to kernel) */
 static __global__ void __launch_bounds__(256) k_exact_init(int *cnt, int *tf, size_t ntf, int32_t *colE, int32_t *colEmin,
@@ -928,8 +942,9 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
     round_pass(r2, 4 * sm_count());
   }
   profile_mark(kPhaseFallback, true, st);
-  chk(launch_pdl(k_fallback<N, CPLX>, dim3((p.n + 31) / 32, (p.m + 7) / 8), dim3(256), 0, st, (size_t)p.m,
-                 (size_t)p.n, (size_t)p.k, A, lda, B, ldb, C, ldc, (const uint8_t *)rowF, (const uint8_t *)colF,
+  const size_t fb_blocks = (size_t)((p.n + 31) / 32) * ((p.m + 7) / 8);
+  chk(launch_pdl(k_fallback<N, CPLX>, dim3((unsigned)std::max<size_t>(1, std::min(fb_blocks, (size_t)2 * sm_count()))), dim3(256), 0, st,
+                 (size_t)p.m, (size_t)p.n, (size_t)p.k, A, lda, B, ldb, C, ldc, (const uint8_t *)rowF, (const uint8_t *)colF,
                  (const int *)cnt, n_fallback));
   profile_mark(kPhaseFallback, false, st);
   if (e != cudaSuccess) return MPB_ERR_CUDA;
