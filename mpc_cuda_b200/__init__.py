@@ -97,6 +97,7 @@ _SIGS = {
     "mpb_batch_gemv_destroy": ([_V], None),
     "mpb_gemm_exact_workspace": ([_I, _S, _S, _S, _I], C.c_size_t),
     "mpb_profile_enable": ([_I], None),
+    "mpb_profile_phases": ([C.c_uint], None),
     "mpb_profile_phase_ms": ([_I], C.c_float),
     "mpb_profile_phase_count": ([_I], C.c_int),
     "mpb_gemm_exact_r": ([_I, _S, _S, _S, _V, _S, _V, _S, _V, _S, _I, _V, _S, _V, _V], C.c_int),

@@ -25,6 +25,7 @@ int sm_count() {
 /* Each recorded interval is an event pair taken from a growing pool; the
  * intervals of every call since mpb_profile_enable(1) are kept and summed. */
 static std::atomic<int> g_profile{0};
+static std::atomic<unsigned> g_profile_mask{~0u}; /* phases that record events */
 static std::mutex g_prof_mu;
 static std::vector<cudaEvent_t> g_pool;
 static size_t g_pool_used = 0;
@@ -42,10 +43,17 @@ static cudaEvent_t next_event() {
 
 void profile_mark(int phase, bool begin, cudaStream_t st) {
   if (!g_profile.load(std::memory_order_relaxed) || phase < 0 || phase >= kPhases) return;
+  if (!((g_profile_mask.load(std::memory_order_relaxed) >> phase) & 1u)) return;
   std::lock_guard<std::mutex> lk(g_prof_mu);
   cudaEvent_t e = next_event();
   if (!e) return;
-  cudaEventRecord(e, st);
+  /* inside a stream capture a plain record only orders the capture; an
+   * external record becomes a node that records the event at every replay */
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+    cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+  else
+    cudaEventRecord(e, st);
   if (begin)
     g_open[phase] = e;
   else if (g_open[phase])
@@ -155,6 +163,11 @@ extern "C" void mpb_profile_enable(int on) {
   g_profile.store(on ? 1 : 0);
 }
 
+extern "C" void mpb_profile_phases(unsigned mask) {
+  using namespace mpb;
+  g_profile_mask.store(mask);
+}
+
 extern "C" float mpb_profile_phase_ms(int phase) {
   using namespace mpb;
   if (phase < 0 || phase >= kPhases) return -1.0f;
@@ -163,8 +176,10 @@ extern "C" float mpb_profile_phase_ms(int phase) {
   double total = 0.0;
   for (auto &iv : g_iv[phase]) {
     float ms = 0.0f;
-    if (cudaEventSynchronize(iv.second) != cudaSuccess) return -1.0f;
-    if (cudaEventElapsedTime(&ms, iv.first, iv.second) != cudaSuccess) return -1.0f;
+    if (cudaEventSynchronize(iv.second) != cudaSuccess || cudaEventElapsedTime(&ms, iv.first, iv.second) != cudaSuccess) {
+      cudaGetLastError(); /* a failed query is this call's answer, not a later launch's error */
+      return -1.0f;
+    }
     total += ms;
   }
   return (float)total;

@@ -334,8 +334,17 @@ int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *e
   CUtensorMap tmA, tmB;
   if (!make_tmap(&tmA, Asl, p.kp, p.m, p.nprod * p.S, BM) || !make_tmap(&tmB, Bsl, p.kp, p.n, p.nprod * p.S, BN))
     return MPB_ERR_CUDA;
-  if (cudaFuncSetAttribute(k_diag_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes) != cudaSuccess)
-    return MPB_ERR_CUDA;
+  /* the shared-memory opt-in, once per device (a call made while a stream is
+   * being captured then issues nothing but the launches) */
+  static std::atomic<unsigned long long> smem_set{0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MPB_ERR_CUDA;
+  if (!((smem_set.load(std::memory_order_acquire) >> dev) & 1ull)) {
+    if (cudaFuncSetAttribute(k_diag_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes) !=
+        cudaSuccess)
+      return MPB_ERR_CUDA;
+    smem_set.fetch_or(1ull << dev, std::memory_order_acq_rel);
+  }
   GemmArgs ga;
   ga.S = p.S;
   ga.nprod = p.nprod;

@@ -327,3 +327,60 @@ def test_tensor_kernel_wait_runs_out_and_reports(orc, mpb):
     C, st = run_exact(mpb, prec, m, n, k, A, B, sp_bits=16)
     assert st.tolist() == [0, 0]
     assert orc.mismatches(prec, C, orc.gemm_exact(prec, m, n, k, A, k, B, n, impl="mp"))[0] == 0
+
+
+@pytest.mark.parametrize("cplx", (False, True))
+def test_exact_gemm_graph_capture_replays_bit_exact(mpb, cplx):
+    """The whole exact GEMM call (statistics, slicing, tensor-core passes,
+    rounding, fallback; launched with programmatic stream serialisation) is
+    captured into a CUDA graph and replayed: every replay must give the direct
+    call's result and status, including a row outside the spread budget that
+    the fallback computes inside the graph (real case)."""
+    import torch
+
+    prec = 256 if cplx else 512
+    m, n, k = 70, 96, 96  # n, k multiples of 32: no padding
+    if cplx:
+        rng = np.random.default_rng(0xCA97)
+        A = synth.interleave_complex(prec, synth.random_elems(rng, prec, m * k, -6, 6),
+                                     synth.random_elems(rng, prec, m * k, -6, 6))
+        B = synth.interleave_complex(prec, synth.random_elems(rng, prec, k * n, -6, 6),
+                                     synth.random_elems(rng, prec, k * n, -6, 6))
+    else:
+        A = rand_aos(prec, m * k, 0xCA98, -6, 6).reshape(m, k, -1)
+        A[3, 5] = rand_aos(prec, 1, 0xCA9A, -60, -60, 0.0)[0]  # row 3 spreads 54+ bits: fallback
+        A = A.reshape(m * k, -1)
+        B = rand_aos(prec, k * n, 0xCA99, -6, 6)
+    dA = to_dev(layout.aos_to_vec(prec, A, cplx))
+    dB = to_dev(layout.aos_to_vec(prec, B, cplx))
+    ws = torch.empty(mpb.gemm_exact_workspace(prec, m, n, k, 16, cplx), dtype=torch.uint8, device="cuda")
+    ref, refst = mpb.empty(prec, m * n, cplx), torch.zeros(2, dtype=torch.int32, device="cuda")
+    out, outst = mpb.empty(prec, m * n, cplx), torch.zeros(2, dtype=torch.int32, device="cuda")
+    s = torch.cuda.Stream()
+
+    def call(C, st):
+        mpb.gemm_exact(prec, m, n, k, dA, k, dB, n, C, n, sp_bits=16, workspace=ws, status=st, cplx=cplx, stream=s)
+
+    with torch.cuda.stream(s):
+        call(ref, refst)  # direct call (also the per-device set-up, outside the capture)
+    torch.cuda.synchronize()
+    L = mpb.lib()
+    L.mpb_profile_enable(1)  # the phase events become nodes of the graph
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        call(out, outst)
+    for _ in range(2):
+        out.zero_()
+        outst.fill_(-1)
+        torch.cuda.synchronize()
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(out, ref)
+        assert outst.tolist() == refst.tolist()
+    # the tensor-core phase of the last replay, timed by the captured events
+    assert L.mpb_profile_phase_count(2) == 1 and L.mpb_profile_phase_ms(2) > 0.0
+    L.mpb_profile_enable(0)
+    assert refst[1].item() == 0
+    if not cplx:
+        assert refst[0].item() >= 1  # the row outside the budget went to the fallback
+    del g
