@@ -325,6 +325,19 @@ static bool make_tmap(CUtensorMap *tm, void *base, int kp, int rows, int planes,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+bool make_plane_tmap(CUtensorMap *tm, const int32_t *base, size_t entries, int nl, int nprod, size_t plane_elems,
+                     size_t q_elems, int box_x) {
+  auto fn = encode_fn();
+  if (!fn || nl < 1 || nl > 256 || box_x < 4 || box_x > 256) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)entries, (cuuint64_t)nl, (cuuint64_t)nprod};
+  const cuuint64_t strides[2] = {(cuuint64_t)plane_elems * 4u, (cuuint64_t)q_elems * 4u};
+  const cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)nl, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_INT32, 3, (void *)base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 /* failure-path test: consumed by the next tensor-core launch of the process */
 static std::atomic<int> g_inject{0};
 static std::atomic<long long> g_inject_wait_ns{0};

@@ -8,6 +8,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "common.cuh"
@@ -408,6 +409,11 @@ struct GemmArgs {
  * mpb_status */
 int launch_diag_gemm(const Plan &p, int8_t *Asl, int8_t *Bsl, int32_t *D, int *err, int dl, int dh,
                      const int *tiles, const int *ntiles, cudaStream_t st);
+/* a TMA map over the computed diagonal planes of a rounding pass (exact_gemm.cu):
+ * int32 [nprod][nl][entries] from base, plane stride plane_elems, product
+ * stride q_elems, box {box_x entries, nl planes, 1 product}, no swizzle */
+bool make_plane_tmap(CUtensorMap *tm, const int32_t *base, size_t entries, int nl, int nprod, size_t plane_elems,
+                     size_t q_elems, int box_x);
 
 /* ------------------------------------------------------------------ *
  * 4. exact recombination and the single rounding
@@ -626,6 +632,86 @@ __device__ __forceinline__ void mark_tile(const RoundPass &rp, int i, int j) {
  * words under the leading bit from the thread's shared-memory slot.  Complex
  * outputs read each product's planes once and form both components:
  * re = T0 - T1, im = T2 - T0 - T1.  Every loop is unrolled at compile time. */
+/* One entry (i, j) of a rounding pass from its planes: ld(q, jc) returns
+ * plane d_first + jc of product q for this entry (jc < nl; plane indices at
+ * or past nl are read clamped and count as zero, so every load of a batch is
+ * unconditional and all are in flight before any is used).  svr / svi: this
+ * thread's shared-memory word slots. */
+template <int N, int XL, bool CPLX, class Ld>
+__device__ __forceinline__ void round_entry(int i, int j, size_t idx, int nl, int SP, const int32_t *rowE,
+                                            const int32_t *colE, uint8_t *C, size_t ldc, const RoundPass &rp,
+                                            uint32_t *svr, uint32_t *svi, Ld ld) {
+  constexpr int QJ = round_geo<N, XL>::QJ;
+  constexpr int BATCH = CPLX ? 8 : 16; /* a multiple of 4 */
+  /* BATCH planes of every product in flight, then their BATCH/4 words:
+   * word w = carry + sum of planes 4w..4w+3 (each < 2^31, times 2^(8j)),
+   * low 32 bits kept, the rest carried on */
+  uint32_t vr[QJ], vi[CPLX ? QJ : 1];
+  long long cr = 0, ci = 0;
+#pragma unroll
+  for (int j0 = 0; j0 < 4 * QJ; j0 += BATCH) {
+    int32_t t0v[BATCH], t1v[CPLX ? BATCH : 1], t2v[CPLX ? BATCH : 1];
+#pragma unroll
+    for (int jj = 0; jj < BATCH; ++jj) {
+      /* unconditional loads (a plane past the last one re-reads the last,
+       * then counts as 0), so they can all be issued before any is used */
+      const bool in = j0 + jj < nl;
+      const int jc = min(j0 + jj, nl - 1);
+      const int32_t x0 = ld(0, jc);
+      t0v[jj] = in ? x0 : 0;
+      if (CPLX) {
+        const int32_t x1 = ld(1, jc), x2 = ld(2, jc);
+        t1v[jj] = in ? x1 : 0;
+        t2v[jj] = in ? x2 : 0;
+      }
+    }
+#pragma unroll
+    for (int w4 = 0; w4 < BATCH / 4; ++w4) {
+      const int w = j0 / 4 + w4;
+      if (w < QJ) {
+        long long tr = cr, ti = ci;
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const long long scale = 1LL << (8 * jj);
+          const long long t0 = t0v[4 * w4 + jj];
+          if (CPLX) {
+            const long long t1 = t1v[4 * w4 + jj], t2 = t2v[4 * w4 + jj];
+            tr += (t0 - t1) * scale;
+            ti += (t2 - t0 - t1) * scale;
+          } else {
+            tr += t0 * scale;
+          }
+        }
+        vr[w] = (uint32_t)tr;
+        cr = tr >> 32;
+        if (CPLX) {
+          vi[w] = (uint32_t)ti;
+          ci = ti >> 32;
+        }
+      }
+    }
+  }
+  const long lsb = (long)rowE[i] + colE[j] - 2L * (32 * N) - 2L * SP + 8L * rp.d_first;
+  /* an all-zero row or column has all-zero digits: its sum is exactly 0 */
+  const long cert =
+      (rowE[i] == kExpZero || colE[j] == kExpZero || rp.cert < 0) ? -1 : rp.cert - 8L * rp.d_first;
+  fval<N> re;
+  bool ok = round_regs<N, QJ>(re, vr, svr, lsb, cert);
+  fval<N> im;
+  if (CPLX) ok = round_regs<N, QJ>(im, *reinterpret_cast<uint32_t(*)[QJ]>(vi), svi, lsb, cert) && ok;
+  if (!rp.flagged_only) {
+    rp.ef[idx] = ok ? 0 : 1;
+    if (!ok) {
+      mark_tile(rp, i, j);
+      return;
+    }
+  }
+  if (CPLX)
+    store_celem<N>(C, (size_t)i * ldc + j, re, im);
+  else
+    store_elem<N>(C, (size_t)i * ldc + j, re);
+}
+
 template <int N, int XL, bool CPLX>
 __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
                                   round_geo<N, XL>::template threads<CPLX>() == 128 ? 4 : 8)
@@ -639,7 +725,6 @@ __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
   __shared__ uint32_t swords[T * SW * (CPLX ? 2 : 1)];
   uint32_t *svr = swords + threadIdx.x * SW * (CPLX ? 2 : 1);
   uint32_t *svi = svr + SW;
-  constexpr int BATCH = CPLX ? 8 : 16; /* a multiple of 4 */
   static_assert(4 * QJ >= J, "words must cover the planes");
   const size_t total = pass_total(rp, m, n), plane = rp.dplane;
   const int ndiag = 2 * S - 1;
@@ -653,74 +738,72 @@ __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
       if (!rp.flagged_only) rp.ef[idx] = 0;
       continue;
     }
-    /* BATCH planes of every product in flight, then their BATCH/4 words:
-     * word w = carry + sum of planes 4w..4w+3 (each < 2^31, times 2^(8j)),
-     * low 32 bits kept, the rest carried on */
-    uint32_t vr[QJ], vi[CPLX ? QJ : 1];
-    long long cr = 0, ci = 0;
     const int32_t *base = D + (size_t)rp.d_first * plane + idx;
-#pragma unroll
-    for (int j0 = 0; j0 < 4 * QJ; j0 += BATCH) {
-      int32_t t0v[BATCH], t1v[CPLX ? BATCH : 1], t2v[CPLX ? BATCH : 1];
-#pragma unroll
-      for (int jj = 0; jj < BATCH; ++jj) {
-        /* unconditional loads (a plane past the last one re-reads the last,
-         * then counts as 0), so they can all be issued before any is used */
-        const bool in = j0 + jj < nl;
-        const size_t off = (size_t)min(j0 + jj, nl - 1) * plane;
-        const int32_t x0 = base[off];
-        t0v[jj] = in ? x0 : 0;
-        if (CPLX) {
-          const int32_t x1 = base[qstride + off], x2 = base[2 * qstride + off];
-          t1v[jj] = in ? x1 : 0;
-          t2v[jj] = in ? x2 : 0;
-        }
-      }
-#pragma unroll
-      for (int w4 = 0; w4 < BATCH / 4; ++w4) {
-        const int w = j0 / 4 + w4;
-        if (w < QJ) {
-          long long tr = cr, ti = ci;
-#pragma unroll
-          for (int jj = 0; jj < 4; ++jj) {
-            const long long scale = 1LL << (8 * jj);
-            const long long t0 = t0v[4 * w4 + jj];
-            if (CPLX) {
-              const long long t1 = t1v[4 * w4 + jj], t2 = t2v[4 * w4 + jj];
-              tr += (t0 - t1) * scale;
-              ti += (t2 - t0 - t1) * scale;
-            } else {
-              tr += t0 * scale;
-            }
-          }
-          vr[w] = (uint32_t)tr;
-          cr = tr >> 32;
-          if (CPLX) {
-            vi[w] = (uint32_t)ti;
-            ci = ti >> 32;
-          }
-        }
-      }
+    round_entry<N, XL, CPLX>(i, j, idx, nl, SP, rowE, colE, C, ldc, rp, svr, svi,
+                             [&](int q, int jc) { return base[(size_t)q * qstride + (size_t)jc * plane]; });
+  }
+}
+
+/* The first pass with the planes staged in shared memory: the T consecutive
+ * entries of a block-step arrive for every computed plane (nprod x nl rows
+ * of T int32) by one TMA load per product (no multicast) on the block's
+ * mbarrier, and round_entry reads them from shared memory.  The plane bytes
+ * then stream from HBM while the other blocks of the SM compute, instead of
+ * each thread waiting on its own plane loads.  The wait is bounded: on
+ * timeout the block records code 6 in err, waits (bounded) for its copy and
+ * returns.  Entries past the end of C are zero-filled by the copy and not
+ * visited. */
+template <int N, int XL, bool CPLX>
+__global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(), 3)
+    k_exact_round_tma(const __grid_constant__ CUtensorMap tmD, int m, int n, int SP, const int32_t *rowE,
+                      const int32_t *colE, const uint8_t *rowF, const uint8_t *colF, uint8_t *C, size_t ldc,
+                      RoundPass rp, int nl, long long wait_ns, int *err) {
+  pdl_wait(); /* launched after the previous stage with launch_pdl */
+  constexpr int QJ = round_geo<N, XL>::QJ;
+  constexpr int SW = QJ | 1;
+  constexpr int T = round_geo<N, XL>::template threads<CPLX>();
+  constexpr int NP = CPLX ? 3 : 1;
+  __shared__ uint32_t swords[T * SW * (CPLX ? 2 : 1)];
+  __shared__ uint64_t bar;
+  extern __shared__ uint8_t dyn_raw[];
+  const int32_t *stage = (const int32_t *)(((uintptr_t)dyn_raw + 127) & ~(uintptr_t)127);
+  uint32_t *svr = swords + threadIdx.x * SW * (CPLX ? 2 : 1);
+  uint32_t *svi = svr + SW;
+  if (threadIdx.x == 0) {
+    sm100::mbar_init(&bar, 1);
+    sm100::fence_barrier_init();
+  }
+  __syncthreads();
+  const size_t total = (size_t)m * n;
+  const uint32_t bytes = (uint32_t)NP * (uint32_t)nl * T * 4u;
+  volatile int never = 0;
+  uint32_t phase = 0u;
+  for (size_t c0 = (size_t)blockIdx.x * T; c0 < total; c0 += (size_t)gridDim.x * T) {
+    if (threadIdx.x == 0) {
+      sm100::mbar_arrive_expect_tx(&bar, bytes);
+      for (int q = 0; q < NP; ++q)
+        sm100::tma_load_3d((void *)(stage + (size_t)q * nl * T), &tmD, (int)c0, 0, q, &bar);
     }
-    const long lsb = (long)rowE[i] + colE[j] - 2L * (32 * N) - 2L * SP + 8L * rp.d_first;
-    /* an all-zero row or column has all-zero digits: its sum is exactly 0 */
-    const long cert =
-        (rowE[i] == kExpZero || colE[j] == kExpZero || rp.cert < 0) ? -1 : rp.cert - 8L * rp.d_first;
-    fval<N> re;
-    bool ok = round_regs<N, QJ>(re, vr, svr, lsb, cert);
-    fval<N> im;
-    if (CPLX) ok = round_regs<N, QJ>(im, *reinterpret_cast<uint32_t(*)[QJ]>(vi), svi, lsb, cert) && ok;
-    if (!rp.flagged_only) {
-      rp.ef[idx] = ok ? 0 : 1;
-      if (!ok) {
-        mark_tile(rp, i, j);
-        continue;
+    const bool ok = sm100::mbar_wait(&bar, phase, &never, (uint64_t)wait_ns);
+    if (__syncthreads_or(ok ? 0 : 1)) {
+      if (threadIdx.x == 0) {
+        atomicCAS(err, 0, 6);
+        sm100::mbar_wait(&bar, phase, &never, (uint64_t)wait_ns); /* the copy still in flight */
       }
+      return;
     }
-    if (CPLX)
-      store_celem<N>(C, (size_t)i * ldc + j, re, im);
-    else
-      store_elem<N>(C, (size_t)i * ldc + j, re);
+    phase ^= 1u;
+    const size_t u = c0 + threadIdx.x;
+    int i, j;
+    size_t idx;
+    if (u < total && pass_entry(rp, m, n, u, i, j, idx)) {
+      if (rowF[i] || colF[j]) /* computed by the fallback */
+        rp.ef[idx] = 0;
+      else
+        round_entry<N, XL, CPLX>(i, j, idx, nl, SP, rowE, colE, C, ldc, rp, svr, svi,
+                                 [&](int q, int jc) { return stage[((size_t)q * nl + jc) * T + threadIdx.x]; });
+    }
+    __syncthreads(); /* every row read before the next copy overwrites the stage */
   }
 }
 
@@ -915,7 +998,40 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
   auto round_pass = [&](const RoundPass &r, int grid_cap) {
     const int32_t *Dc = D, *rE = rowE, *cE = colE;
     const uint8_t *rF = rowF, *cF = colF;
-    if (p.P == 1 && !r.flagged_only && 2 * p.S - 1 - r.d_first <= round_geo<N, XL>::J) {
+    const int nl = 2 * p.S - 1 - r.d_first;
+    constexpr int TT = round_geo<N, XL>::template threads<CPLX>();
+    const size_t stage_bytes = (size_t)p.nprod * nl * TT * 4;
+    CUtensorMap tmD;
+    /* shared-memory stage of the TMA rounding pass, at most: measured on B200,
+     * a 37 KB stage (real 1024^3 at 512 bits, 72 planes) took the pass from
+     * 133.7 to 95.7 us, a 61 KB one (complex 512^3 at 256 bits, 3 x 40
+     * planes, two blocks per SM) from 43.2 to 54.0 us, so larger stages keep
+     * the kernel that loads its planes itself */
+    constexpr size_t kStageMax = 48 * 1024;
+    if (p.P == 1 && !r.flagged_only && nl <= round_geo<N, XL>::J && nl <= 256 && stage_bytes <= kStageMax &&
+        make_plane_tmap(&tmD, D + (size_t)r.d_first * r.dplane, (size_t)p.m * p.n, nl, p.nprod, r.dplane,
+                        (size_t)(2 * p.S - 1) * r.dplane, TT)) {
+      /* planes staged in shared memory by TMA (the first pass of the usual sizes) */
+      auto kern = k_exact_round_tma<N, XL, CPLX>;
+      const int dsm = (int)stage_bytes + 128;
+      /* the opt-in for the largest stage, once per device (the 48 KB default
+       * covers static and dynamic shared memory together) */
+      static std::atomic<unsigned long long> smem_set{0};
+      int dev = 0;
+      chk(cudaGetDevice(&dev));
+      if (dev >= 0 && dev < 64 && !((smem_set.load(std::memory_order_acquire) >> dev) & 1ull)) {
+        const cudaError_t ra =
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageMax + 128);
+        chk(ra);
+        if (ra == cudaSuccess) smem_set.fetch_or(1ull << dev, std::memory_order_acq_rel);
+      }
+      int per = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, TT, dsm) != cudaSuccess || per < 1) per = 1;
+      const size_t chunks = ((size_t)p.m * p.n + TT - 1) / TT;
+      const int g = (int)std::min(chunks, (size_t)per * sm_count());
+      chk(launch_pdl(kern, dim3(g), dim3(TT), (size_t)dsm, st, tmD, p.m, p.n, p.SP, rE, cE, rF, cF, C, ldc, r, nl,
+                     (long long)sm100::kWaitNs, cnt + 1));
+    } else if (p.P == 1 && !r.flagged_only && nl <= round_geo<N, XL>::J) {
       constexpr int T = round_geo<N, XL>::template threads<CPLX>();
       const int g = std::min(grid_cap, grid_for(k_exact_round<N, XL, CPLX>, T, (size_t)p.m * p.n));
       chk(launch_pdl(k_exact_round<N, XL, CPLX>, dim3(g), dim3(T), 0, st, p.m, p.n, p.S, p.SP, Dc, rE, cE, rF, cF,
