@@ -298,91 +298,126 @@ __device__ __forceinline__ void aligned_twos(uint32_t (&w)[N + XL + 1], const fv
  * each XOR 0x80 (adding 128 to every byte produces exactly the carries of
  * the digit-by-digit recoding: byte b plus carry becomes b - 256, carry 1,
  * when it reaches 128).  One carry chain for U, then every digit is a byte
- * extraction.  For |V| < 2^(8S-2) every digit above S-1 is zero, so put(s, d)
- * is called for s < S only. */
-template <int L1, typename F>
-__device__ __forceinline__ void twos_digits(const uint32_t (&w)[L1], int S, F put) {
-  uint32_t u[L1];
+ * extraction.  For |V| < 2^(8S-2) every digit above S-1 is zero, so only
+ * the digits s < S are written. */
+template <int L1>
+__device__ __forceinline__ void offset_words(uint32_t (&u)[L1], const uint32_t (&w)[L1]) {
   uint32_t cf = 0;
   u[0] = add_cc(w[0], 0x80808080u, cf);
 #pragma unroll
   for (int i = 1; i < L1; ++i) u[i] = addc_cc(w[i], 0x80808080u, cf);
-#pragma unroll
-  for (int s = 0; s < 4 * L1; ++s)
-    if (s < S) put(s, (int8_t)(((u[s >> 2] >> (8 * (s & 3))) & 0xffu) ^ 0x80u));
-}
-/* the digit stream of one element for product q: 0 (real / re part),
- * 1 (im), 2 (re + im) */
-template <int N, int XL, bool CPLX, typename F>
-__device__ __forceinline__ void element_digits(const fval<N> &re, const fval<N> &im, int32_t E, int SP, int S,
-                                               int q, F put) {
-  uint32_t w[N + XL + 1];
-  aligned_twos<N, XL>(w, q == 1 ? im : re, E, SP);
-  if (CPLX && q == 2) {
-    uint32_t v[N + XL + 1];
-    aligned_twos<N, XL>(v, im, E, SP);
-    uint32_t c = 0;
-#pragma unroll
-    for (int i = 0; i <= N + XL; ++i) {
-      const uint64_t t = (uint64_t)w[i] + v[i] + c;
-      w[i] = (uint32_t)t;
-      c = (uint32_t)(t >> 32);
-    }
-  }
-  twos_digits(w, S, put);
 }
 
-/* A (m x k, tiles) -> A_sl[q*S+s][i][kp]; thread per (i, kk), kk < kp (zero padding) */
+/* elements per thread of the slicing kernels: E consecutive k of one row of
+ * A (column of B), so every digit plane gets E bytes per store (one 32-bit
+ * store for E = 4) while the E elements' offset words fit in registers */
+template <int N, bool CPLX>
+struct slice_geo {
+  static constexpr int E = CPLX ? (N <= 8 ? 4 : N <= 16 ? 2 : 1) : (N <= 16 ? 4 : N <= 32 ? 2 : 1);
+};
+
+/* The digit planes of E consecutive elements for product q (0: the real
+ * part, 1: the imaginary part, 2: re + im): ld(e, re, im) loads element e
+ * (zero when it is padding or flagged); the digits of plane s go to
+ * dst + s * plane, E bytes (E-aligned), element e in byte e. */
+template <int N, int XL, bool CPLX, int E, typename Ld>
+__device__ __forceinline__ void slice_elements(Ld ld, int32_t Eexp, int SP, int S, int q, int8_t *dst, size_t plane) {
+  constexpr int L1 = N + XL + 1;
+  uint32_t u[E][L1];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    fval<N> re, im;
+    ld(e, re, im);
+    uint32_t w[L1];
+    aligned_twos<N, XL>(w, q == 1 ? im : re, Eexp, SP);
+    if (CPLX && q == 2) {
+      uint32_t v[L1];
+      aligned_twos<N, XL>(v, im, Eexp, SP);
+      uint32_t c = 0;
+#pragma unroll
+      for (int i = 0; i < L1; ++i) {
+        const uint64_t t = (uint64_t)w[i] + v[i] + c;
+        w[i] = (uint32_t)t;
+        c = (uint32_t)(t >> 32);
+      }
+    }
+    offset_words<L1>(u[e], w);
+  }
+#pragma unroll
+  for (int s = 0; s < 4 * L1; ++s) {
+    if (s >= S) continue; /* predicated: the loop stays unrolled, u in registers */
+    const int wd = s >> 2, b = s & 3;
+    int8_t *o = dst + (size_t)s * plane;
+    if (E == 4) {
+      /* byte b of each element's word, elements 0..3 in bytes 0..3 */
+      const uint32_t t01 = __byte_perm(u[0][wd], u[E > 1 ? 1 : 0][wd], (uint32_t)(b | ((4 + b) << 4)));
+      const uint32_t t23 = __byte_perm(u[E > 2 ? 2 : 0][wd], u[E > 3 ? 3 : 0][wd], (uint32_t)(b | ((4 + b) << 4)));
+      *(uint32_t *)o = __byte_perm(t01, t23, 0x5410u) ^ 0x80808080u;
+    } else if (E == 2) {
+      const uint32_t t01 = __byte_perm(u[0][wd], u[E > 1 ? 1 : 0][wd], (uint32_t)(b | ((4 + b) << 4)));
+      *(uint16_t *)o = (uint16_t)((t01 ^ 0x8080u) & 0xffffu);
+    } else {
+      *o = (int8_t)(((u[0][wd] >> (8 * b)) & 0xffu) ^ 0x80u);
+    }
+  }
+}
+
+/* A (m x k, tiles) -> A_sl[q*S+s][i][kp]; thread per (i, E consecutive kk),
+ * kk < kp (zero padding) */
 template <int N, int XL, bool CPLX>
 __global__ void __launch_bounds__(128) k_slice_a(int m, int k, int kp, const uint8_t *A, size_t lda, int SP, int S,
                                                  const int32_t *rowE, const uint8_t *rowF, int8_t *Asl) {
   pdl_wait(); /* launched after the previous stage with launch_pdl */
-  const size_t total = (size_t)m * kp, plane = (size_t)m * kp;
+  constexpr int E = slice_geo<N, CPLX>::E;
+  const size_t groups = (size_t)kp / E, total = (size_t)m * groups, plane = (size_t)m * kp;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(idx / kp), kk = (int)(idx % kp);
-    fval<N> re, im;
-    set_zero(im);
-    if (kk < k && !rowF[i])
-      load_any<N, CPLX>(re, im, A, (size_t)i * lda + kk);
-    else
-      set_zero(re);
-    const int32_t E = rowE[i];
-    int8_t *dst = Asl + (size_t)i * kp + kk;
+    const int i = (int)(idx / groups), kk0 = (int)(idx % groups) * E;
+    const bool live = !rowF[i];
+    const int32_t Ex = rowE[i];
+    int8_t *dst = Asl + (size_t)i * kp + kk0;
 #pragma unroll 1
-    for (int q = 0; q < (CPLX ? 3 : 1); ++q) {
-      int8_t *dq = dst + (size_t)q * S * plane;
-      element_digits<N, XL, CPLX>(re, im, E, SP, S, q, [&](int s, int8_t d) { dq[(size_t)s * plane] = d; });
-    }
+    for (int q = 0; q < (CPLX ? 3 : 1); ++q)
+      slice_elements<N, XL, CPLX, E>(
+          [&](int e, fval<N> &re, fval<N> &im) {
+            set_zero(im);
+            if (live && kk0 + e < k)
+              load_any<N, CPLX>(re, im, A, (size_t)i * lda + kk0 + e);
+            else
+              set_zero(re);
+          },
+          Ex, SP, S, q, dst + (size_t)q * S * plane, plane);
   }
 }
 
-/* B (k x n, tiles) -> B_sl[q*S+s][j][kp]: thread per (j, kk) with kk running
- * fastest across the lanes, so each digit plane is written as 32-byte rows
- * (one byte per lane) and no staging is needed; the lanes' element loads
- * come from 32 rows of B (16-byte pieces whose tile neighbours are read by
- * the warps of columns j +- 1 soon after, from L2). */
+/* B (k x n, tiles) -> B_sl[q*S+s][j][kp]: thread per (j, E consecutive kk)
+ * with kk running fastest across the lanes, so each digit plane is written as
+ * 32E-byte rows (E bytes per lane) and no staging is needed; the lanes'
+ * element loads come from rows of B (16-byte pieces whose tile neighbours
+ * are read by the warps of columns j +- 1 soon after, from L2). */
 template <int N, int XL, bool CPLX>
 __global__ void __launch_bounds__(128) k_slice_b(int n, int k, int kp, const uint8_t *B, size_t ldb, int SP, int S,
                                                  const int32_t *colE, const uint8_t *colF, int8_t *Bsl) {
   pdl_wait(); /* launched after the previous stage with launch_pdl */
-  const size_t total = (size_t)n * kp, plane = (size_t)n * kp;
+  constexpr int E = slice_geo<N, CPLX>::E;
+  const size_t groups = (size_t)kp / E, total = (size_t)n * groups, plane = (size_t)n * kp;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (size_t)gridDim.x * blockDim.x) {
-    const int j = (int)(idx / kp), kk = (int)(idx % kp);
-    fval<N> re, im;
-    set_zero(im);
-    if (kk < k && !colF[j])
-      load_any<N, CPLX>(re, im, B, (size_t)kk * ldb + j);
-    else
-      set_zero(re);
-    const int32_t E = colE[j];
-    int8_t *dst = Bsl + (size_t)j * kp + kk;
+    const int j = (int)(idx / groups), kk0 = (int)(idx % groups) * E;
+    const bool live = !colF[j];
+    const int32_t Ex = colE[j];
+    int8_t *dst = Bsl + (size_t)j * kp + kk0;
 #pragma unroll 1
-    for (int q = 0; q < (CPLX ? 3 : 1); ++q) {
-      int8_t *dq = dst + (size_t)q * S * plane;
-      element_digits<N, XL, CPLX>(re, im, E, SP, S, q, [&](int s, int8_t d) { dq[(size_t)s * plane] = d; });
-    }
+    for (int q = 0; q < (CPLX ? 3 : 1); ++q)
+      slice_elements<N, XL, CPLX, E>(
+          [&](int e, fval<N> &re, fval<N> &im) {
+            set_zero(im);
+            if (live && kk0 + e < k)
+              load_any<N, CPLX>(re, im, B, (size_t)(kk0 + e) * ldb + j);
+            else
+              set_zero(re);
+          },
+          Ex, SP, S, q, dst + (size_t)q * S * plane, plane);
   }
 }
 
@@ -983,9 +1018,9 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
                  p.n, colE, (const int32_t *)colEmin, colF, cnt));
   profile_mark(kPhaseStats, false, st);
   profile_mark(kPhaseSlice, true, st);
-  chk(launch_pdl(k_slice_a<N, XL, CPLX>, dim3(grid_for(k_slice_a<N, XL, CPLX>, 128, (size_t)p.m * p.kp)), dim3(128),
+  chk(launch_pdl(k_slice_a<N, XL, CPLX>, dim3(grid_for(k_slice_a<N, XL, CPLX>, 128, (size_t)p.m * p.kp / slice_geo<N, CPLX>::E)), dim3(128),
                  0, st, p.m, p.k, p.kp, A, lda, p.SP, p.S, (const int32_t *)rowE, (const uint8_t *)rowF, Asl));
-  chk(launch_pdl(k_slice_b<N, XL, CPLX>, dim3(grid_for(k_slice_b<N, XL, CPLX>, 128, (size_t)p.n * p.kp)), dim3(128),
+  chk(launch_pdl(k_slice_b<N, XL, CPLX>, dim3(grid_for(k_slice_b<N, XL, CPLX>, 128, (size_t)p.n * p.kp / slice_geo<N, CPLX>::E)), dim3(128),
                  0, st, p.n, p.k, p.kp, B, ldb, p.SP, p.S, (const int32_t *)colE, (const uint8_t *)colF, Bsl));
   profile_mark(kPhaseSlice, false, st);
   if (e != cudaSuccess || launch_status() != MPB_OK) return MPB_ERR_CUDA;
