@@ -1040,7 +1040,8 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
     /* shared-memory stage of the TMA rounding pass, at most: measured on B200,
      * a 37 KB stage (real 1024^3 at 512 bits, 72 planes) took the pass from
      * 133.7 to 95.7 us, a 61 KB one (complex 512^3 at 256 bits, 3 x 40
-     * planes, two blocks per SM) from 43.2 to 54.0 us, so larger stages keep
+     * planes, two blocks per SM) from 43.2 to 54.0 us, and in chunks of 64
+     * entries (30 KB, five blocks per SM) to 51.8 us, so larger stages keep
      * the kernel that loads its planes itself */
     constexpr size_t kStageMax = 48 * 1024;
     if (p.P == 1 && !r.flagged_only && nl <= round_geo<N, XL>::J && nl <= 256 && stage_bytes <= kStageMax &&
