@@ -658,20 +658,19 @@ __device__ __forceinline__ void mark_tile(const RoundPass &rp, int i, int j) {
   if (atomicExch(rp.tf + tile, 1) == 0) rp.tiles[atomicAdd(rp.ntiles, 1)] = tile;
 }
 
-/* First pass with a single k-part (P == 1) and at most J planes from
- * d_first on: the planes of output idx are loaded BATCH at a time and
+/* One entry (i, j) of a single-part (P == 1) rounding pass over at most J
+ * planes from d_first on.  ld(q, jc) returns plane d_first + jc of product q
+ * for this entry (jc < nl; plane indices at or past nl are read clamped and
+ * count as zero, so every load of a batch is unconditional and all are in
+ * flight before any is used).  The planes are taken BATCH at a time and
  * streamed into 32-bit words with an int64 carry -- plane d_first + j lands
  * in word j/4, byte j%4.  The words hold the sum divided by 256^d_first, so
  * the LSB exponent and the certification bound move up by 8 d_first bits
  * instead of the words moving.  round_regs rounds them, reading the few
- * words under the leading bit from the thread's shared-memory slot.  Complex
- * outputs read each product's planes once and form both components:
- * re = T0 - T1, im = T2 - T0 - T1.  Every loop is unrolled at compile time. */
-/* One entry (i, j) of a rounding pass from its planes: ld(q, jc) returns
- * plane d_first + jc of product q for this entry (jc < nl; plane indices at
- * or past nl are read clamped and count as zero, so every load of a batch is
- * unconditional and all are in flight before any is used).  svr / svi: this
- * thread's shared-memory word slots. */
+ * words under the leading bit from this thread's shared-memory slots svr /
+ * svi.  Complex outputs read each product's planes once and form both
+ * components: re = T0 - T1, im = T2 - T0 - T1.  Every loop is unrolled at
+ * compile time. */
 template <int N, int XL, bool CPLX, class Ld>
 __device__ __forceinline__ void round_entry(int i, int j, size_t idx, int nl, int SP, const int32_t *rowE,
                                             const int32_t *colE, uint8_t *C, size_t ldc, const RoundPass &rp,
@@ -747,6 +746,8 @@ __device__ __forceinline__ void round_entry(int i, int j, size_t idx, int nl, in
     store_elem<N>(C, (size_t)i * ldc + j, re);
 }
 
+/* The single-part pass with each thread loading its own planes (every
+ * size; the second pass over the marked tiles too). */
 template <int N, int XL, bool CPLX>
 __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
                                   round_geo<N, XL>::template threads<CPLX>() == 128 ? 4 : 8)
