@@ -746,8 +746,8 @@ __device__ __forceinline__ void round_entry(int i, int j, size_t idx, int nl, in
     store_elem<N>(C, (size_t)i * ldc + j, re);
 }
 
-/* The single-part pass with each thread loading its own planes (every
- * size; the second pass over the marked tiles too). */
+/* The single-part first pass with each thread loading its own planes (the
+ * sizes whose shared-memory stage would exceed the TMA kernel's limit). */
 template <int N, int XL, bool CPLX>
 __global__ void __launch_bounds__(round_geo<N, XL>::template threads<CPLX>(),
                                   round_geo<N, XL>::template threads<CPLX>() == 128 ? 4 : 8)
