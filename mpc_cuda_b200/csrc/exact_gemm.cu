@@ -426,15 +426,22 @@ static int exact_entry(int cplx, int prec, size_t m, size_t n, size_t k, const v
                        size_t ldb, void *C, size_t ldc, int sp_bits, void *workspace, size_t ws_bytes, int *status,
                        void *stream) {
   if (!prec_ok(prec)) return MPB_ERR_PREC;
-  if (m == 0 || n == 0) return MPB_OK;
+  /* an empty product still reports: nothing fell back, no kernel error */
+  auto clear_status = [&]() -> int {
+    if (status && cudaMemsetAsync(status, 0, 2 * sizeof(int), as_stream(stream)) != cudaSuccess) return MPB_ERR_CUDA;
+    return MPB_OK;
+  };
+  if (m == 0 || n == 0) return clear_status();
   if (m > (1u << 24) || n > (1u << 24) || k > (1u << 24)) return MPB_ERR_SIZE;
   if (ldc % 32 || ldc < n) return MPB_ERR_LD;
   if (k > 0 && (lda % 32 || lda < k || ldb % 32 || ldb < n)) return MPB_ERR_LD;
   if (!C || (k > 0 && (!A || !B))) return MPB_ERR_NULL;
   if (!aligned16(C) || (k > 0 && (!aligned16(A) || !aligned16(B)))) return MPB_ERR_ALIGN;
-  if (k == 0) /* empty sums: +0 everywhere */
-    return cplx ? mpb_gemm_c(prec, m, n, 0, nullptr, 32, nullptr, 32, C, ldc, stream)
-                : mpb_gemm_r(prec, m, n, 0, nullptr, 32, nullptr, 32, C, ldc, stream);
+  if (k == 0) { /* empty sums: +0 everywhere */
+    const int rc = cplx ? mpb_gemm_c(prec, m, n, 0, nullptr, 32, nullptr, 32, C, ldc, stream)
+                        : mpb_gemm_r(prec, m, n, 0, nullptr, 32, nullptr, 32, C, ldc, stream);
+    return rc != MPB_OK ? rc : clear_status();
+  }
   exact::Plan p;
   if (!exact::make_plan(prec, m, n, k, sp_bits, cplx, p)) return MPB_ERR_ARG;
   if (!workspace || ws_bytes < p.total) return MPB_ERR_WORKSPACE;
@@ -507,13 +514,20 @@ extern "C" int mpb_gemm_exact_r_static(int prec, size_t m, size_t n, size_t k, c
                                        const void *B, size_t ldb, void *C, size_t ldc, int sp_bits, int *status,
                                        void *stream) {
   if (!prec_ok(prec)) return MPB_ERR_PREC;
-  if (m == 0 || n == 0) return MPB_OK;
+  auto clear_status = [&]() -> int { /* an empty product reports no fallback, no error */
+    if (status && cudaMemsetAsync(status, 0, 2 * sizeof(int), as_stream(stream)) != cudaSuccess) return MPB_ERR_CUDA;
+    return MPB_OK;
+  };
+  if (m == 0 || n == 0) return clear_status();
   if (m > (1u << 24) || n > (1u << 24) || k > (1u << 24)) return MPB_ERR_SIZE;
   if (ldc % 32 || ldc < n) return MPB_ERR_LD;
   if (k > 0 && (lda % 32 || lda < k || ldb % 32 || ldb < n)) return MPB_ERR_LD;
   if (!C || (k > 0 && (!A || !B))) return MPB_ERR_NULL;
   if (!aligned16(C) || (k > 0 && (!aligned16(A) || !aligned16(B)))) return MPB_ERR_ALIGN;
-  if (k == 0) return mpb_gemm_r(prec, m, n, 0, nullptr, 32, nullptr, 32, C, ldc, stream);
+  if (k == 0) {
+    const int rc = mpb_gemm_r(prec, m, n, 0, nullptr, 32, nullptr, 32, C, ldc, stream);
+    return rc != MPB_OK ? rc : clear_status();
+  }
   exact::Plan p;
   if (!exact::make_plan(prec, m, n, k, sp_bits, 0, p)) return MPB_ERR_ARG;
   if (p.total > kStaticScratchBytes) return MPB_ERR_SIZE; /* larger than the static scratch area */

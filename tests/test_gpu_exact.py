@@ -384,3 +384,32 @@ def test_exact_gemm_graph_capture_replays_bit_exact(mpb, cplx):
     if not cplx:
         assert refst[0].item() >= 1  # the row outside the budget went to the fallback
     del g
+
+
+@pytest.mark.parametrize("cplx", (False, True))
+def test_exact_gemm_empty_dimensions(mpb, cplx):
+    """k = 0: every entry is the empty sum +0; m = 0: nothing to do.  Both
+    report a clean status (no fallback, no error) into a reused status word."""
+    import torch
+
+    prec, m, n, ldc = 256, 5, 40, 64
+    rng = np.random.default_rng(0xE0)
+    zero_parts = (np.zeros((1, prec // 32), np.uint32), np.array([layout.HEAD_ZERO], np.uint32))
+    if cplx:
+        C0 = synth.interleave_complex(prec, synth.random_elems(rng, prec, m * ldc, -4, 4),
+                                      synth.random_elems(rng, prec, m * ldc, -4, 4))
+        zero = synth.interleave_complex(prec, zero_parts, zero_parts)[0]
+    else:
+        C0 = layout.aos_from_parts(prec, *synth.random_elems(rng, prec, m * ldc, -4, 4))
+        zero = layout.aos_from_parts(prec, *zero_parts)[0]
+    C = to_dev(layout.aos_to_vec(prec, C0, cplx))
+    st = torch.full((2,), -7, dtype=torch.int32, device="cuda")
+    mpb.gemm_exact(prec, m, n, 0, None, 32, None, 64, C, ldc, sp_bits=16, status=st, cplx=cplx)
+    torch.cuda.synchronize()
+    assert st.tolist() == [0, 0]
+    got = layout.vec_to_aos(prec, to_host(C), m * ldc, cplx).reshape(m, ldc, -1)[:, :n]
+    assert (got == zero).all(), "k = 0 must give +0 in every entry"
+    st.fill_(-7)
+    mpb.gemm_exact(prec, 0, n, 8, None, 32, None, 64, C, ldc, sp_bits=16, status=st, cplx=cplx)
+    torch.cuda.synchronize()
+    assert st.tolist() == [0, 0]
