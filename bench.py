@@ -168,10 +168,10 @@ class AxpyWorkload:
         from mpc_cuda_b200 import layout, synth
 
         if self.cplx:
-            a, x, y = synth.axpy_c1024(seed=self.seed + 1000 * rank, n=self.n, prec=self.prec)
+            a, x, y = synth.axpy_c1024(seed=shard_seed(self.seed, rank), n=self.n, prec=self.prec)
             conv = lambda p: synth.interleave_complex(self.prec, *p)  # noqa: E731
         else:
-            a, x, y = synth.axpy_r256(seed=self.seed + 1000 * rank, n=self.n, prec=self.prec)
+            a, x, y = synth.axpy_r256(seed=shard_seed(self.seed, rank), n=self.n, prec=self.prec)
             conv = lambda p: layout.aos_from_parts(self.prec, *p)  # noqa: E731
         return conv(a), conv(x), conv(y)
 
@@ -329,7 +329,7 @@ class GemmWorkload:
 
         from mpc_cuda_b200 import synth
 
-        a, b = self.gen(seed=(0x5EED5 if self.cplx else 0x5EED3) + 1000 * rank)
+        a, b = self.gen(seed=shard_seed(0x5EED5 if self.cplx else 0x5EED3, rank))
         if self.cplx:
             return synth.interleave_complex(self.prec, *a), synth.interleave_complex(self.prec, *b)
         return layout.aos_from_parts(self.prec, *a), layout.aos_from_parts(self.prec, *b)
@@ -494,7 +494,7 @@ class GemvBatchWorkload:
     def make_host(self, rank):
         from mpc_cuda_b200 import layout, synth
 
-        probs, pools = synth.gemv_batch(seed=self.seed + 1000 * rank, count=self.count)
+        probs, pools = synth.gemv_batch(seed=shard_seed(self.seed, rank), count=self.count)
         aos = {p: tuple(layout.aos_from_parts(p, *P[k]) for k in ("A", "x", "y")) for p, P in pools.items()}
         return probs, aos
 
@@ -679,7 +679,7 @@ class DivSqrtWorkload(AxpyWorkload):
     def make_host(self, rank):
         from mpc_cuda_b200 import layout, synth
 
-        rng = np.random.default_rng(self.seed + 1000 * rank)
+        rng = np.random.default_rng(shard_seed(self.seed, rank))
         lo, hi = {"div": (-40, 40), "sqrt": (-40, 40), "exp": (-3, 3), "log": (-20, 20), "sin": (-5, 5)}[self.op]
         x = synth.random_elems(rng, self.prec, self.n, lo, hi)
         y = synth.random_elems(rng, self.prec, self.n, lo, hi)
@@ -788,7 +788,7 @@ class CfnWorkload(AxpyWorkload):
     def make_host(self, rank):
         from mpc_cuda_b200 import synth
 
-        rng = np.random.default_rng(self.seed + 1000 * rank)
+        rng = np.random.default_rng(shard_seed(self.seed, rank))
         re = synth.random_elems(rng, self.prec, self.n, -3, 3)
         im = synth.random_elems(rng, self.prec, self.n, -3, 3)
         x = synth.interleave_complex(self.prec, re, im)
@@ -988,6 +988,26 @@ def split_targets(wl):
     raise SystemExit(f"--split: workload {wl.name} has no warp-cooperative form")
 
 
+def shard_seed(base, rank):
+    """Seed of a rank's shard: every rank generates its own operands of the
+    full workload size (weak scaling; no data crosses ranks)."""
+    return base + 1000 * rank
+
+
+def max_over_ranks_of(v, world, device):
+    """The max of v over the ranks of the default process group (the job's
+    time is its slowest rank's); device: the tensor's device for the backend
+    (cuda for NCCL, cpu for gloo)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -1007,11 +1027,7 @@ def run_gpu(args):
             dist.barrier()
 
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(v, world, device)
 
     wl = WORKLOADS[args.workload]()
     wl.with_e2e = not args.no_e2e
