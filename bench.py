@@ -101,6 +101,72 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+class NvmlClocks:
+    """The same SM clock and clock-event reasons nvidia-smi reports, read
+    through NVML by a thread every ~2 ms while the timed regions run (a timed
+    region of 20 GEMM steps lasts ~40 ms, shorter than nvidia-smi's start-up
+    and sampling period).  Read-only: no setting of the GPU is touched."""
+
+    BITS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+            "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+            "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+            "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
+
+    def __init__(self, cuda_index: int):
+        import pynvml
+        import torch
+
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(cuda_index).uuid)
+        try:
+            self.h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(cuda_index)
+        self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        self.samples, self.stop_flag, self.thread = [], False, None
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop_flag:
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)),
+                                     int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def start(self):
+        import threading
+
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        self.stop_flag = True
+        self.thread.join(timeout=5)
+        reasons = set()
+        for _, bits in self.samples:
+            for nm, const in self.BITS.items():
+                if bits & getattr(self.nv, const):
+                    reasons.add(nm)
+        sm = [mhz for mhz, _ in self.samples]
+        try:
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(sm), "source": "NVML, every ~2 ms"}
+
+
+def make_clocks(cuda_index: int):
+    """NVML sampling when the bindings are importable, else nvidia-smi."""
+    try:
+        return NvmlClocks(cuda_index)
+    except Exception:
+        return Clocks(cuda_index)
+
+
 # ------------------------------------------------------------------ helpers
 def pinned_from(np_arr):
     import torch
@@ -1044,7 +1110,7 @@ def run_gpu(args):
         wl.step(i, sp)
     torch.cuda.synchronize()
 
-    clocks = Clocks(local) if rank == 0 else None
+    clocks = make_clocks(local) if rank == 0 else None
     barrier()
     torch.cuda.synchronize()
     if clocks:
@@ -1257,7 +1323,7 @@ def run_dropin(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / reps
 
-    clocks = Clocks(0)
+    clocks = make_clocks(0)
     clocks.start()
     rows = []
     for prec in DROPIN_PRECS:
