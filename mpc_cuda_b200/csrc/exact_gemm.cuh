@@ -166,7 +166,7 @@ __device__ __forceinline__ uint32_t head_of(const uint8_t *base, size_t idx, int
  * block per (32 columns, chunk), and each block folds its partial max / min
  * exponent into colE / colEmin with atomics (initialised to kColNone /
  * kColMinNone by a byte memset).  k_row_stats then finalises the columns. */
-constexpr int kColRows = 128;
+constexpr int kColRows = 32; /* 32-row chunks: a 512 x 512 B is 256 blocks, enough for every SM */
 constexpr int32_t kColNone = (int32_t)0x80808080;    /* memset 0x80: no nonzero entry seen */
 constexpr int32_t kColMinNone = (int32_t)0x7f7f7f7f; /* memset 0x7f */
 template <int N, bool CPLX>
@@ -208,15 +208,17 @@ __global__ void __launch_bounds__(256) k_col_stats(int n, int k, const uint8_t *
   }
 }
 
-/* one warp per row of A: E_i = max exponent of the nonzero entries (both
- * parts of a complex entry); flag the row when some nonzero entry lies more
- * than SP bits below E_i.  The same launch finalises the column statistics:
- * an all-zero column gets kExpZero, a column whose spread exceeds SP is
- * flagged; flagged rows and columns are counted. */
+/* one block of kRowWarps warps per row of A, the warps splitting k: E_i =
+ * max exponent of the nonzero entries (both parts of a complex entry); flag
+ * the row when some nonzero entry lies more than SP bits below E_i.  The same
+ * launch finalises the column statistics: an all-zero column gets kExpZero,
+ * a column whose spread exceeds SP is flagged; flagged rows and columns are
+ * counted. */
+constexpr int kRowWarps = 4;
 template <int N, bool CPLX>
-__global__ void __launch_bounds__(256) k_row_stats(int m, int k, const uint8_t *A, size_t lda, int SP, int32_t *rowE,
-                                                   uint8_t *rowF, int n, int32_t *colE, const int32_t *colEmin,
-                                                   uint8_t *colF, int *count) {
+__global__ void __launch_bounds__(kRowWarps * 32) k_row_stats(int m, int k, const uint8_t *A, size_t lda, int SP,
+                                                              int32_t *rowE, uint8_t *rowF, int n, int32_t *colE,
+                                                              const int32_t *colEmin, uint8_t *colF, int *count) {
   pdl_wait(); /* launched after the previous stage with launch_pdl */
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const int32_t e = colE[j];
@@ -226,16 +228,17 @@ __global__ void __launch_bounds__(256) k_row_stats(int m, int k, const uint8_t *
     colF[j] = flag ? 1 : 0;
     if (flag) atomicAdd(count, 1);
   }
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= m) return;
+  __shared__ int32_t smax[kRowWarps], smin[kRowWarps];
+  const int row = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (row >= m) return; /* block-uniform */
   int32_t emax = kExpZero, emin = 0x7fffffff;
 #pragma unroll 4
-  for (int k0 = 0; k0 < k; k0 += 32) {
+  for (int k0 = w * 32; k0 < k; k0 += kRowWarps * 32) {
     const int kk = k0 + lane;
     if (kk < k) {
 #pragma unroll
       for (int part = 0; part < (CPLX ? 2 : 1); ++part) {
-        const uint32_t h = head_of<N, CPLX>(A, (size_t)warp * lda + kk, part);
+        const uint32_t h = head_of<N, CPLX>(A, (size_t)row * lda + kk, part);
         if (h != kHeadZero) {
           const int32_t e = head_exp(h);
           emax = max(emax, e);
@@ -250,9 +253,18 @@ __global__ void __launch_bounds__(256) k_row_stats(int m, int k, const uint8_t *
     emin = min(emin, __shfl_xor_sync(0xffffffffu, emin, o));
   }
   if (lane == 0) {
-    rowE[warp] = emax;
+    smax[w] = emax;
+    smin[w] = emin;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < kRowWarps; ++q) {
+      emax = max(emax, smax[q]);
+      emin = min(emin, smin[q]);
+    }
+    rowE[row] = emax;
     const bool flag = emax != kExpZero && (long)emax - emin > SP;
-    rowF[warp] = flag ? 1 : 0;
+    rowF[row] = flag ? 1 : 0;
     if (flag) atomicAdd(count, 1);
   }
 }
@@ -1015,7 +1027,8 @@ static int run_impl(const Plan &p, const uint8_t *A, size_t lda, const uint8_t *
   profile_mark(kPhaseStats, true, st);
   chk(launch_pdl(k_col_stats<N, CPLX>, dim3((p.n + 31) / 32, (p.k + kColRows - 1) / kColRows), dim3(256), 0, st,
                  p.n, p.k, B, ldb, colE, colEmin));
-  chk(launch_pdl(k_row_stats<N, CPLX>, dim3((p.m + 7) / 8), dim3(256), 0, st, p.m, p.k, A, lda, p.SP, rowE, rowF,
+  /* one block per row of A; the column finalisation strides over the grid */
+  chk(launch_pdl(k_row_stats<N, CPLX>, dim3(p.m), dim3(kRowWarps * 32), 0, st, p.m, p.k, A, lda, p.SP, rowE, rowF,
                  p.n, colE, (const int32_t *)colEmin, colF, cnt));
   profile_mark(kPhaseStats, false, st);
   profile_mark(kPhaseSlice, true, st);
