@@ -1275,7 +1275,7 @@ def run_kernel_tour(args):
 
 
 # ------------------------------------------------------------------ drop-in user kernels
-DROPIN_PRECS = (64, 96, 128, 160, 256, 288, 512, 1024, 1056, 2048)
+DROPIN_PRECS = (64, 96, 128, 160, 256, 288, 512, 1024, 1056, 2048, 4096)  # 4096: the real kernels only
 
 
 def _uk_lib(path, pre):
@@ -1331,6 +1331,8 @@ def run_dropin(args):
         row = {"prec": prec}
         for kind, n in (("real", 1 << 20), ("complex", 1 << 18)):
             cplx = kind == "complex"
+            if cplx and prec > 2048:
+                continue
             if prec >= 1024:
                 n >>= 2
             X, Y = O.gen_pairs(prec, n, 0xD00D + prec, cplx=cplx)

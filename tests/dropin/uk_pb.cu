@@ -7,8 +7,12 @@
 #endif
 
 namespace uk {
+#if UK_PB > 2048
+UK_REAL_LAUNCHERS(, UK_PB)
+#else
 UK_LAUNCHERS(, UK_PB)
-#if UK_PB != 2048
+#endif
+#if UK_PB < 2048 /* the elementary functions stop below 2048 bits (constant tables) */
 UK_FN_LAUNCHERS(, UK_PB)
 #endif
 }  // namespace uk

@@ -31,9 +31,11 @@ using namespace uk;
 
 #define UK_DECL(PB) UK_LAUNCHERS(extern, PB)
 #define UK_DECL_FN(PB) UK_FN_LAUNCHERS(extern, PB)
+#define UK_DECL_REAL(PB) UK_REAL_LAUNCHERS(extern, PB)
 namespace uk {
 UK_FOR_EACH_PB(UK_DECL)
 UK_FOR_EACH_FN_PB(UK_DECL_FN)
+UK_FOR_EACH_REAL_ONLY_PB(UK_DECL_REAL)
 }  // namespace uk
 
 namespace {
@@ -60,6 +62,14 @@ int launched() { return cudaGetLastError() == cudaSuccess ? 0 : -3; }
     default: return -1;                                                                  \
   }                                                                                      \
   return launched();
+#define UK_DISPATCH_REAL(P, CALL)                                                         \
+  switch (P) {                                                                           \
+    UK_CASE(64, CALL) UK_CASE(96, CALL) UK_CASE(128, CALL) UK_CASE(160, CALL)            \
+    UK_CASE(256, CALL) UK_CASE(288, CALL) UK_CASE(512, CALL) UK_CASE(1024, CALL)         \
+    UK_CASE(1056, CALL) UK_CASE(2048, CALL) UK_CASE(4096, CALL)                          \
+    default: return -1;                                                                  \
+  }                                                                                      \
+  return launched();
 #define UK_DISPATCH_FN(P, CALL)                                                           \
   switch (P) {                                                                           \
     UK_CASE(64, CALL) UK_CASE(96, CALL) UK_CASE(128, CALL) UK_CASE(160, CALL)            \
@@ -76,7 +86,7 @@ int launched() { return cudaGetLastError() == cudaSuccess ? 0 : -3; }
 extern "C" {
 int UK(axpy_r)(int prec, long n, const void *a, const void *x, const void *y, void *z, int grid, int block,
                void *stream) {
-  UK_DISPATCH(prec, (run_axpy_r<PB>(UK_LAUNCH, n, a, x, y, z)))
+  UK_DISPATCH_REAL(prec, (run_axpy_r<PB>(UK_LAUNCH, n, a, x, y, z)))
 }
 int UK(axpy_c)(int prec, long n, const void *a, const void *x, const void *y, void *z, int grid, int block,
                void *stream) {
@@ -84,7 +94,7 @@ int UK(axpy_c)(int prec, long n, const void *a, const void *x, const void *y, vo
 }
 int UK(axpy_d)(int prec, long n, double a, const double *X, const double *Y, double *O, int grid, int block,
                void *stream) {
-  UK_DISPATCH(prec, (run_axpy_d<PB>(UK_LAUNCH, n, a, X, Y, O)))
+  UK_DISPATCH_REAL(prec, (run_axpy_d<PB>(UK_LAUNCH, n, a, X, Y, O)))
 }
 int UK(caxpy_d)(int prec, long n, double ar, double ai, const double *XR, const double *XI, const double *YR,
                 const double *YI, double *OR, double *OI, int grid, int block, void *stream) {
@@ -92,7 +102,7 @@ int UK(caxpy_d)(int prec, long n, double ar, double ai, const double *XR, const 
 }
 int UK(matmul_r)(int prec, int m, int n, int k, const void *A, int lda, const void *B, int ldb, void *C, int ldc,
                  int grid, int block, void *stream) {
-  UK_DISPATCH(prec, (run_matmul_r<PB>(UK_LAUNCH, m, n, k, A, lda, B, ldb, C, ldc)))
+  UK_DISPATCH_REAL(prec, (run_matmul_r<PB>(UK_LAUNCH, m, n, k, A, lda, B, ldb, C, ldc)))
 }
 int UK(matmul_c)(int prec, int m, int n, int k, const void *A, int lda, const void *B, int ldb, void *C, int ldc,
                  int grid, int block, void *stream) {

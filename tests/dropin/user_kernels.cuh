@@ -121,16 +121,21 @@ void run_div(int g, int b, cudaStream_t s, long n, const void *x, const void *y,
 }
 
 /* the launchers of one precision, declared (UK_EXTERN) or instantiated (UK_INST) */
-#define UK_LAUNCHERS(KW, PB)                                                                                   \
+/* the real kernels (every precision, 4096 bits included) */
+#define UK_REAL_LAUNCHERS(KW, PB)                                                                              \
   KW template void run_axpy_r<PB>(int, int, cudaStream_t, long, const void *, const void *, const void *, void *); \
-  KW template void run_axpy_c<PB>(int, int, cudaStream_t, long, const void *, const void *, const void *, void *); \
   KW template void run_axpy_d<PB>(int, int, cudaStream_t, long, double, const double *, const double *, double *); \
+  KW template void run_matmul_r<PB>(int, int, cudaStream_t, int, int, int, const void *, int, const void *, int, \
+                                    void *, int);
+/* the complex kernels: up to 2048 bits (at 4096 their unrolled products take
+ * many minutes to compile) */
+#define UK_CPLX_LAUNCHERS(KW, PB)                                                                              \
+  KW template void run_axpy_c<PB>(int, int, cudaStream_t, long, const void *, const void *, const void *, void *); \
   KW template void run_caxpy_d<PB>(int, int, cudaStream_t, long, double, double, const double *, const double *, \
                                    const double *, const double *, double *, double *);                       \
-  KW template void run_matmul_r<PB>(int, int, cudaStream_t, int, int, int, const void *, int, const void *, int, \
-                                    void *, int);                                                              \
   KW template void run_matmul_c<PB>(int, int, cudaStream_t, int, int, int, const void *, int, const void *, int, \
                                     void *, int);
+#define UK_LAUNCHERS(KW, PB) UK_REAL_LAUNCHERS(KW, PB) UK_CPLX_LAUNCHERS(KW, PB)
 /* the elementary functions stop at 1056 bits: at 2048 the reference's
  * runtime-indexed guard-precision arrays take very long to compile */
 #define UK_FN_LAUNCHERS(KW, PB)                                                   \
@@ -138,6 +143,7 @@ void run_div(int g, int b, cudaStream_t s, long n, const void *x, const void *y,
   KW template void run_div<PB>(int, int, cudaStream_t, long, const void *, const void *, void *);
 
 #define UK_FOR_EACH_PB(X) X(64) X(96) X(128) X(160) X(256) X(288) X(512) X(1024) X(1056) X(2048)
+#define UK_FOR_EACH_REAL_ONLY_PB(X) X(4096)
 #define UK_FOR_EACH_FN_PB(X) X(64) X(96) X(128) X(160) X(256) X(288) X(512) X(1024) X(1056)
 
 }  // namespace uk

@@ -128,6 +128,32 @@ def test_user_matmul_sequential_k(orc, uk, prec):
     assert bad == 0, f"complex matmul PB={prec}: {bad} differ (first {first})"
 
 
+def test_user_real_kernels_at_4096_bits(orc, uk, refuk):
+    """Above 2048 bits (the reference benchmarks 4096 bits and up,
+    demos/bench_3way.cu:167-169): the real AXPY and the sequential-k real
+    matmul through the drop-in header at 4096 bits, bit for bit against MPFR,
+    and the same source built against the reference's header agreeing."""
+    prec = 4096
+    d = _Dev()
+    es = orc.elem_bytes(prec)
+    n = 600
+    X, Y = orc.gen_pairs(prec, n, 0xA1 + prec)
+    a = orc.gen_pairs(prec, 1, 0xA2 + prec)[0]
+    want = orc.axpy(prec, a, X, Y, impl="mp")
+    for L, pre in ((uk, "uk_"), (refuk, "refuk_")):
+        z = d.out(n * es)
+        _call(L, pre + "axpy_r", prec, n, d.put(a), d.put(X), d.put(Y), z.data_ptr(), 0, 128, None)
+        bad, first = orc.mismatches(prec, d.get(z, (n, es)), want)
+        assert bad == 0, f"{pre}axpy_r PB={prec}: {bad} differ from MPFR (first {first})"
+    m, nn, k = 4, 8, 9
+    A, _ = orc.gen_pairs(prec, m * k, 0xB1 + prec)
+    B, _ = orc.gen_pairs(prec, k * nn, 0xB2 + prec)
+    c = d.out(m * nn * es)
+    _call(uk, "uk_matmul_r", prec, m, nn, k, d.put(A), k, d.put(B), nn, c.data_ptr(), nn, 0, 64, None)
+    bad, first = orc.mismatches(prec, d.get(c, (m * nn, es)), orc.gemm(prec, m, nn, k, A, k, B, nn, impl="mp"))
+    assert bad == 0, f"real matmul PB={prec}: {bad} differ (first {first})"
+
+
 @pytest.mark.parametrize("prec", FN_PRECS)
 def test_user_exp_and_div(orc, mpb, uk, prec):
     d = _Dev()
